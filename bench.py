@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Throughput of the Smc-CAT likelihood hot path on B200.
+
+Workload (default): the FP64 GTR+G4+I configuration, 48 taxa x 2,000 sites,
+4 gamma categories, 256 particles, seeded synthetic data. One step = one full
+likelihood refresh (the reference's refreshLikelihood(true) after
+copyFromSerialized) of every particle: 256 x 2,000 x 4 = 2,048,000
+particle*site*category evaluations.
+
+* ``value``  -- device-timed throughput with the particle states resident in HBM.
+* ``e2e``    -- the same metric through the public C-ABI with host buffers:
+  every step uploads all particle states (smccat_set_particles), refreshes and
+  reads the log-likelihoods back (smccat_get_lnl).
+* ``roofline`` -- the pruning kernel's algorithmic HBM bytes per launch over its
+  CUDA-event duration, against the measured copy bandwidth.
+* ``cpu_baseline`` -- the FP64 oracle (the reference's algorithm with its
+  OpenMP-over-particles structure) on a bounded sample, all host threads.
+
+``--impl reference`` times that CPU implementation alone as the reference arm.
+Multi-GPU (torchrun): every rank holds its own 256 particles; no collective in
+the data path (weak scaling); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "smc-cat_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle*site*cat lik evals/s"
+UNIT = "evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=int, default=32,
+                    help="particles per CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def algorithmic_cost(T: int, R: int):
+    """Per (particle, site, category) unit of one full refresh, stored-CL design.
+
+    Bytes: each of the T-1 internal nodes writes its 20-state FP64 partial and
+    one FP64 cumulative log-scaler; each of the T-2 internal non-root nodes is
+    read back once by its parent (partial + scaler); each tip contributes its
+    1-byte code per site (shared by the R categories).
+    Flops (the reference's count): two dense 20x20 child mat-vecs, the
+    Hadamard product and the rescale per internal node: (T-1) * 1660.
+    """
+    b = (T - 1) * (20 * 8 + 8) + (T - 2) * (20 * 8 + 8) + T / R
+    f = (T - 1) * (2 * 800 + 60)
+    return b, f
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dgemm_peak_tflops():
+    """cuBLAS FP64 GEMM throughput as the measured FP64 ceiling."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def cpu_baseline(cfg, codes, st, n_sample, min_seconds=10.0):
+    """Time the oracle's OpenMP full refresh on a bounded particle sample."""
+    import oracle
+    from smccat import discretize_gamma
+    n = min(n_sample, st["parent"].shape[0])
+    sl = slice(0, n)
+    rates = np.stack([discretize_gamma(s, cfg.R) for s in st["shape"][sl]])
+    args = (codes, st["parent"][sl], st["branch"][sl], st["base"][sl], st["num_classes"][sl],
+            st["logits"][sl], st["assign"][sl], st["pinv"][sl], rates)
+    threads = oracle.max_threads()
+    oracle.lnl_batch(*args, nthreads=threads)  # warm-up
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        oracle.lnl_batch(*args, nthreads=threads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds:
+            break
+    units = reps * n * cfg.S * cfg.R
+    return {"value": units / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} particles x {cfg.S} sites x {cfg.R} categories, full refresh, "
+                      f"{reps} repetitions in {el:.1f} s (FP64 oracle, OpenMP over particles)"}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU implementation of the path on the host cores."""
+    if rank != 0:
+        return
+    import oracle
+    from smccat import discretize_gamma, workload
+    cfg = workload.CONFIGS[args.config]
+    rng = np.random.default_rng(cfg.seed)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    n = min(args.cpu_sample, cfg.particles)
+    st = workload.make_particles(cfg, n, rng)
+    rates = np.stack([discretize_gamma(s, cfg.R) for s in st["shape"]])
+    a = (codes, st["parent"], st["branch"], st["base"], st["num_classes"], st["logits"],
+         st["assign"], st["pinv"], rates)
+    threads = oracle.max_threads()
+    for _ in range(args.warmup):
+        oracle.lnl_batch(*a, nthreads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.lnl_batch(*a, nthreads=threads)
+    el = time.perf_counter() - t0
+    value = args.steps * n * cfg.S * cfg.R / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg.name, "taxa": cfg.T, "sites": cfg.S, "rates": cfg.R,
+                   "particles_per_step": n, "model": "GTR+G4+I" if args.config == 2 else cfg.name},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n} particles x {cfg.S} sites x {cfg.R} categories per step "
+                                   "(FP64 oracle restating the reference's refreshLikelihood(true), "
+                                   "OpenMP over particles)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import smccat
+    from smccat import workload
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    cfg = workload.CONFIGS[args.config]
+    rng = np.random.default_rng(cfg.seed)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    prng = np.random.default_rng(cfg.seed * 1000 + rank)
+    st = workload.make_particles(cfg, cfg.particles, prng)
+    n = cfg.particles
+    eng = smccat.Engine(codes, cfg.R, n, max_classes=st["logits"].shape[1], lg=cfg.lg,
+                        invar=cfg.invar, cat=cfg.cat, device=local)
+    load = lambda: eng.set_particles(0, st["parent"], st["branch"], st["base"],  # noqa: E731
+                                     st["num_classes"], st["logits"], st["assign"], st["pinv"],
+                                     st["shape"])
+    load()
+    eng.refresh(full=True)
+    stream = torch.cuda.ExternalStream(eng.stream_ptr, device=torch.device("cuda", local))
+    units_per_step = n * cfg.S * cfg.R
+
+    # ---- device-resident value --------------------------------------------
+    for _ in range(args.warmup):
+        eng.refresh(full=True)
+    barrier()
+    eng.set_profiling(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        eng.refresh(full=True)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    prof = eng.profile()
+    eng.set_profiling(False)
+
+    # ---- e2e through the C-ABI with host buffers ----------------------------
+    lnl_host = None
+    eng.set_profiling(False)
+    for _ in range(2):
+        load()
+        eng.refresh(full=True)
+        lnl_host = eng.lnl()
+    barrier()
+    eng.set_profiling(False)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    f0.record(stream)
+    for _ in range(args.steps):
+        load()
+        eng.refresh(full=True)
+        lnl_host = eng.lnl()
+    f1.record(stream)
+    f1.synchronize()
+    barrier()
+    ms_e2e = f0.elapsed_time(f1)
+    prof_e2e = eng.profile()
+    assert np.all(np.isfinite(lnl_host))
+
+    times = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    ms, ms_e2e = times.tolist()
+    total_units = units_per_step * args.steps * world
+    value = total_units / (ms * 1e-3)
+    e2e_value = total_units / (ms_e2e * 1e-3)
+
+    if rank == 0:
+        b_unit, f_unit = algorithmic_cost(cfg.T, cfg.R)
+        prune_ms = prof["ms"]["prune"] / max(prof["launches"]["prune"], 1)
+        bytes_per_launch = b_unit * units_per_step
+        achieved = bytes_per_launch / (prune_ms * 1e-3) / 1e9
+        peak, peak_kind = measured_peaks()
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "prune_fp64_traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                tj = json.load(f)
+            if tj.get("workload") == cfg.name:
+                traffic = tj.get("dram_bytes_per_launch")
+        try:
+            fp64_peak = dgemm_peak_tflops()
+        except Exception:
+            fp64_peak = None
+        fp64_achieved = f_unit * units_per_step / (prune_ms * 1e-3) / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": cfg.name, "taxa": cfg.T, "sites": cfg.S, "rates": cfg.R,
+                       "particles_per_gpu": n, "model": "GTR+G4+I" if args.config == 2 else cfg.name,
+                       "step": "full refresh of every particle (refreshLikelihood(true))",
+                       "l2": "inputs larger than L2 (CL buffers %.1f GB per GPU)" % (eng.device_bytes / 1e9),
+                       "parallelism": f"particles sharded, {world} GPU(s), no collective"},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": prof_e2e["h2d_bytes"] // args.steps,
+                    "d2h_bytes_per_step": prof_e2e["d2h_bytes"] // args.steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "prune_kernel<4>", "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "avg_launch_ms": prune_ms},
+            "fp64": {"achieved_tflops": fp64_achieved, "dgemm_peak_tflops": fp64_peak,
+                     "frac": (fp64_achieved / fp64_peak) if fp64_peak else None},
+            "kernel_ms_per_step": {k: v / args.steps for k, v in prof["ms"].items()},
+            "gpu_launches": sum(prof["launches"].values()),
+            "clocks": clk,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(cfg, codes, st, args.cpu_sample)
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+/*
+ * smccat.h -- C-ABI of the B200 likelihood engine for Smc-CAT.
+ *
+ * One context (smccat_ctx) holds, on one GPU, a batch of SMC particles over a
+ * fixed alignment: their tree, model parameters, conditional-likelihood (CL)
+ * buffers, transition matrices and per-class spectral data. The calls below
+ * replace the reference's per-particle C++ likelihood interface
+ * (class Particle, src/analysis/Particle.hpp:48-125) with batched calls over a
+ * range of particles [first, first + count).
+ *
+ * Conventions
+ *   - Every call returns an int status: SMCCAT_OK (0) or one of the error
+ *     codes below; smccat_last_error() gives a one-line message. The reference
+ *     exits the process on bad input instead (Alignment.cpp:79-96, Tree.cpp:104,
+ *     main.cpp:158-174).
+ *   - The caller owns every host array; the context owns all device memory.
+ *   - Calls on one context are not thread-safe; each context uses one CUDA
+ *     stream. Contexts on different devices are independent.
+ *   - Trees are rooted and binary, flattened as a parent array over
+ *     2T-1 nodes: tips 0..T-1 (taxon order of the alignment), internal nodes
+ *     T..2T-2, parent[root] = -1 (the reference's node-id convention,
+ *     Tree.cpp:61-74). branch[n] is the length of the edge above node n.
+ *   - Residue codes are the reference's alignment codes (Alignment.cpp:7-31):
+ *     0-19 = ARNDCQEGHILKMFPSTWYV, 20 = '-', 21 = 'X', 22 = '?'.
+ */
+#ifndef SMCCAT_H
+#define SMCCAT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SMCCAT_OK        0
+#define SMCCAT_EINVAL    1  /* bad argument or inconsistent particle state   */
+#define SMCCAT_ECUDA     2  /* a CUDA runtime call failed                   */
+#define SMCCAT_ENOMEM    3  /* device or host allocation failed / too large */
+#define SMCCAT_ESTATE    4  /* call out of protocol order                   */
+#define SMCCAT_ENUMERIC  5  /* a likelihood came out NaN                     */
+#define SMCCAT_ENODEV    6  /* no usable CUDA device                         */
+
+/* model_flags */
+#define SMCCAT_MODEL_LG     1  /* LG exchangeabilities (else GTR, inferred)  */
+#define SMCCAT_MODEL_INVAR  2  /* +I invariant-site mixture                  */
+#define SMCCAT_MODEL_CAT    4  /* Dirichlet-process (CAT) class mixture      */
+
+/* precision */
+#define SMCCAT_PREC_FP64    0  /* plain FP64 pruning                         */
+
+/* refresh modes */
+#define SMCCAT_REFRESH_DIRTY 0 /* refreshLikelihood(false): dirty nodes only */
+#define SMCCAT_REFRESH_FULL  1 /* refreshLikelihood(true): everything        */
+
+typedef struct smccat_ctx smccat_ctx;
+
+typedef struct smccat_config {
+    int32_t num_taxa;       /* T >= 3                                          */
+    int32_t num_sites;      /* S >= 1                                          */
+    int32_t num_rates;      /* R in [1, 8]: discrete-gamma categories          */
+    int32_t max_particles;  /* particles resident on the device at once        */
+    int32_t max_classes;    /* per-particle class capacity (1 without CAT)     */
+    int32_t model_flags;    /* SMCCAT_MODEL_*                                  */
+    int32_t precision;      /* SMCCAT_PREC_*                                   */
+    int32_t device;         /* CUDA device ordinal                             */
+} smccat_config;
+
+/* Library version string, e.g. "smccat-b200 0.1". */
+const char* smccat_version(void);
+
+/* Message for the last error raised on this thread. */
+const char* smccat_last_error(void);
+
+/* discretizeGamma (src/core/Miscellaneous.hpp:22-37): the R midpoint
+ * quantiles (2i+1)/(2R) of Gamma(shape, scale 1/shape), rescaled to mean 1.
+ * Host-only; needs no device. */
+int smccat_discretize_gamma(double shape, int32_t num_rates, double* out);
+
+/* The 190 LG exchangeabilities in the reference's lower-triangle order
+ * (src/analysis/RateMatrices.hpp:7-111): (i, j) for i = 1..19, j < i. The
+ * reference feeds these raw values as the base vector of LG runs
+ * (Particle.cpp:84-94). Host-only. */
+int smccat_lg_exchangeabilities(double* out190);
+
+/* Create a context over the alignment `codes` [T][S] (row-major, taxon-major).
+ * Replaces the data half of Particle::Particle (Particle.cpp:21-73): tip
+ * encoding and the invariant-site flags are derived once and shared by all
+ * particles. */
+int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** out);
+
+int smccat_destroy(smccat_ctx* ctx);
+
+/* Device bytes the context holds. */
+int smccat_device_bytes(const smccat_ctx* ctx, uint64_t* bytes);
+
+/* Load full particle states into slots [first, first+count). Replaces
+ * Particle::copyFromSerialized (Particle.cpp:218-300) minus its refresh: the
+ * SerializedParticle fields (SerializedParticle.hpp:8-17) with the Newick
+ * tree given as parent/branch arrays. Arrays are packed per particle:
+ *   parent [count][2T-1], branch [count][2T-1], base [count][190],
+ *   num_classes [count], logits [count][max_classes][20],
+ *   assign [count][S] (class index of each site), pinv [count], shape [count].
+ * The loaded particles are marked fully dirty; call smccat_refresh next. */
+int smccat_set_particles(smccat_ctx* ctx, int32_t first, int32_t count,
+                         const int32_t* parent, const double* branch,
+                         const double* base, const int32_t* num_classes,
+                         const double* logits, const int32_t* assign,
+                         const double* pinv, const double* shape);
+
+/* Read back particle states in the same packed layout (any pointer may be
+ * NULL). Replaces Particle::writeToSerialized (Particle.cpp:302-320). */
+int smccat_get_particles(smccat_ctx* ctx, int32_t first, int32_t count,
+                         int32_t* parent, double* branch, double* base,
+                         int32_t* num_classes, double* logits, int32_t* assign,
+                         double* pinv, double* shape);
+
+/* Recompute the likelihood of particles [first, first+count).
+ * mode SMCCAT_REFRESH_FULL = refreshLikelihood(true): every spectral
+ * decomposition, transition matrix and internal CL is rebuilt.
+ * mode SMCCAT_REFRESH_DIRTY = refreshLikelihood(false): only what the last
+ * edit calls touched (Particle.cpp:537-571); the root reduction always runs.
+ * Returns SMCCAT_ENUMERIC if any likelihood is NaN (the values are still
+ * stored). Replaces Particle::refreshLikelihood (Particle.cpp:530-675). */
+int smccat_refresh(smccat_ctx* ctx, int32_t first, int32_t count, int32_t mode);
+
+/* Copy the current log-likelihoods of [first, first+count) to `out`.
+ * Replaces Particle::lnLikelihood (Particle.cpp:480-482). */
+int smccat_get_lnl(smccat_ctx* ctx, int32_t first, int32_t count, double* out);
+
+/* Per-site log-likelihoods of particle `p` from its last refresh (S values).
+ * The reference keeps no per-site output; this is the parity probe. */
+int smccat_get_site_lnl(smccat_ctx* ctx, int32_t p, double* out);
+
+/* ---- edits that mark dirty state (the proposal side of the moves) ------ */
+
+/* Set branch lengths of `n` nodes of particle p. Marks the transition
+ * matrices of those nodes and the CLs on their paths to the root dirty
+ * (Tree::scaleBranchMove / scaleSubtreeMove, Tree.cpp:553-612). */
+int smccat_set_branch_lengths(smccat_ctx* ctx, int32_t p, int32_t n,
+                              const int32_t* nodes, const double* lengths);
+
+/* Replace the topology of particle p (NNI / SPR, Tree.cpp:625-812). Nodes
+ * whose children changed, and their ancestors, are marked CL-dirty. */
+int smccat_set_topology(smccat_ctx* ctx, int32_t p, const int32_t* parent,
+                        const double* branch);
+
+/* Proportion of invariant sites (Particle::invarMove, Particle.cpp:744-766):
+ * only the root reduction reruns. */
+int smccat_set_pinv(smccat_ctx* ctx, int32_t p, double pinv);
+
+/* Gamma shape (Particle::shapeMove, Particle.cpp:768-783): rates are
+ * re-discretised and every transition matrix and CL is rebuilt. */
+int smccat_set_shape(smccat_ctx* ctx, int32_t p, double shape);
+
+/* Exchangeabilities (190 log-rates) of particle p. Every class is
+ * re-decomposed and everything downstream rebuilt. */
+int smccat_set_base(smccat_ctx* ctx, int32_t p, const double* base);
+
+/* Logits of class k of particle p: that class is re-decomposed and its
+ * transition matrices and every CL rebuilt (STATIONARY_SINGLE,
+ * Particle.cpp:537-548). */
+int smccat_set_class_logits(smccat_ctx* ctx, int32_t p, int32_t k, const double* logits);
+
+/* Accept (mask[i] != 0) or reject (mask[i] == 0) the pending edits of
+ * particles [first, first+count) after a refresh. Accept keeps the new state;
+ * reject restores the previous state and its likelihood. Both are O(nodes)
+ * flag flips on the device -- no buffer copies (the reference copies the whole
+ * rescale buffer, Particle.cpp:343-478). */
+int smccat_accept(smccat_ctx* ctx, int32_t first, int32_t count, const uint8_t* mask);
+
+/* Synchronise the context's stream. */
+int smccat_sync(smccat_ctx* ctx);
+
+/* ---- measurement (no reference counterpart: the reference only has the
+ * compile-time TIME_PROFILE wall-clock prints, Particle.cpp:533-631) ----- */
+
+/* The cudaStream_t the context launches on, so a caller can record its own
+ * CUDA events on it. */
+int smccat_get_stream(smccat_ctx* ctx, void** stream);
+
+#define SMCCAT_KERNEL_SPEC   0
+#define SMCCAT_KERNEL_PMAT   1
+#define SMCCAT_KERNEL_PRUNE  2
+#define SMCCAT_KERNEL_REDUCE 3
+#define SMCCAT_KERNEL_ACCEPT 4
+#define SMCCAT_NUM_KERNELS   5
+
+typedef struct smccat_profile {
+    uint64_t launches[SMCCAT_NUM_KERNELS];  /* kernel launches by kind          */
+    double ms[SMCCAT_NUM_KERNELS];          /* summed CUDA-event durations (ms)
+                                               when timing is enabled, else 0   */
+    uint64_t h2d_bytes;                     /* host->device bytes copied        */
+    uint64_t d2h_bytes;                     /* device->host bytes copied        */
+} smccat_profile;
+
+/* Enable (1) or disable (0) per-launch CUDA-event timing; resets counters. */
+int smccat_set_profiling(smccat_ctx* ctx, int32_t enable);
+
+/* Counters since the last smccat_set_profiling call (synchronises). */
+int smccat_get_profile(smccat_ctx* ctx, smccat_profile* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SMCCAT_H */

@@ -1,0 +1,42 @@
+// Kernel launch interface of the B200 likelihood engine (host <-> device).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "smccat_internal.h"
+
+namespace smccat {
+
+struct Dims {
+    int T, S, Spad, R, N, NI, Kmax;
+};
+
+struct PruneArgs {
+    Dims d;
+    int first;        // first particle of the refresh range (hdr index base)
+    int tile_begin;   // first global tile of the range
+    const Tile* tiles;
+    const PartHdr* hdr;
+    const NodeJob* nodes;
+    const uint8_t* codes;
+    const int32_t* perm;
+    const double* Pm;
+    const double* spec;
+    const uint8_t* sws;
+    const double* isinv;
+    const int32_t* invchar;
+    double* CL;       // written and re-read inside one launch: never via the nc path
+    double* LSC;
+    double* site_lnl;
+    double* partial;
+};
+
+cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d, cudaStream_t st);
+cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, const uint8_t* sws,
+                        const double* spec, double* Pm, const Dims& d, cudaStream_t st);
+cudaError_t launch_prune(const PruneArgs& a, int ntiles, cudaStream_t st);
+cudaError_t launch_reduce(const int32_t* tile_off, const double* partial, const PartHdr* hdr, int first,
+                          int count, double* lnl, int* status, cudaStream_t st);
+cudaError_t launch_accept(double* lnl, double* lnl_old, const uint8_t* mask, int first, int count,
+                          cudaStream_t st);
+
+}  // namespace smccat

@@ -1,0 +1,73 @@
+// Shared host/device definitions of the B200 likelihood engine.
+//
+// Device layout (one context = one batch of particles on one GPU):
+//   codes   [T][S]                      uint8 alignment codes (shared)
+//   perm    [P][S]                      slot -> site, sites grouped by class
+//   CL      [P][T-1][2][20][R][Spad]    internal-node partials, 2 workspaces,
+//                                       state-major so a warp of 32 slots
+//                                       reads 256 contiguous bytes per state
+//   LSC     [P][T-1][2][R][Spad]        cumulative log scale of each node's
+//                                       subtree (own scaler + children's)
+//   Pm      [P][Kmax][N][2][R][21][20]  transposed transition matrices: row j
+//                                       holds column j of P, row 20 holds the
+//                                       row sums (P applied to an all-ones
+//                                       tip vector for gap / X / ?)
+//   spec    [P][Kmax][2][SPEC_STRIDE]   eigenvalues, left/right factors, pi
+// Every workspace index (CL, P, spectral) is chosen by the host mirror and
+// shipped in the per-refresh plan, so accept/reject never touches the device.
+#pragma once
+#include <stdint.h>
+
+namespace smccat {
+
+constexpr int kStates = 20;
+constexpr int kBase = 190;
+constexpr int kPRows = 21;                      // 20 columns of P + row sums
+constexpr int kPBlock = kPRows * kStates;       // 420 doubles per (node, rate)
+constexpr int kMaxRates = 8;
+constexpr int kTileSites = 64;                  // sites per pruning CTA
+constexpr int kSpecStride = 20 + 400 + 400 + 20 + 8;  // lam, L, Rm, pi, pad
+
+// Offsets inside one spectral record.
+constexpr int kSpecLam = 0;
+constexpr int kSpecL = 20;
+constexpr int kSpecRm = 420;
+constexpr int kSpecPi = 820;
+
+struct PartHdr {
+    int32_t node_off;   // first NodeJob of this particle in the plan
+    int32_t node_cnt;   // dirty internal nodes, post-order, root last
+    int32_t root;       // root node id
+    int32_t root_ws;    // CL workspace of the root after this refresh
+    int32_t active;     // 0: particle not part of this refresh
+    int32_t num_classes;
+    int32_t pad0, pad1;
+    double pinv;
+    double rates[kMaxRates];
+};
+
+// One dirty internal node. ws bits: 0 out CL ws, 1 child1 CL ws, 2 child2
+// CL ws, 3 child1 P ws, 4 child2 P ws.
+struct NodeJob {
+    int32_t node, c1, c2, ws;
+};
+
+// Rebuild the transition matrices of one node (all classes, all rates).
+struct PJob {
+    int32_t p, node, pws, pad;
+    double t;           // branch length
+};
+
+// Re-decompose one class.
+struct SpecJob {
+    int32_t p, k, sws, pad;
+    double base[kBase];
+    double logits[kStates];
+};
+
+// A pruning tile: up to kTileSites consecutive slots of one class.
+struct Tile {
+    int32_t p, k, slot0, nslots;
+};
+
+}  // namespace smccat

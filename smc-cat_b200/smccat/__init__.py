@@ -1,0 +1,276 @@
+"""Python binding of the B200 Smc-CAT likelihood engine (ctypes over the C-ABI).
+
+Everything here calls ``lib/libsmccat.so`` through the functions declared in
+``include/smccat.h``; there is no Python or CPU fallback. Importing works
+without a GPU (the library loads, host-only helpers run); creating an
+:class:`Engine` needs a CUDA device and raises :class:`SmccatError` otherwise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG_DIR, "lib", "libsmccat.so")
+HEADER_PATH = os.path.join(os.path.dirname(_PKG_DIR), "include", "smccat.h")
+
+OK, EINVAL, ECUDA, ENOMEM, ESTATE, ENUMERIC, ENODEV = range(7)
+MODEL_LG, MODEL_INVAR, MODEL_CAT = 1, 2, 4
+PREC_FP64 = 0
+REFRESH_DIRTY, REFRESH_FULL = 0, 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_up = ctypes.POINTER(ctypes.c_uint8)
+_i32 = ctypes.c_int32
+
+
+class SmccatError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"smccat error {code}: {msg}")
+        self.code = code
+
+
+KERNEL_NAMES = ("spec", "pmat", "prune", "reduce", "accept")
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_uint64 * 5), ("ms", ctypes.c_double * 5),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64)]
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("num_taxa", _i32), ("num_sites", _i32), ("num_rates", _i32),
+                ("max_particles", _i32), ("max_classes", _i32), ("model_flags", _i32),
+                ("precision", _i32), ("device", _i32)]
+
+
+_lib = None
+
+
+def build() -> str:
+    """Compile libsmccat.so in-tree with the package Makefile."""
+    subprocess.run(["make", "-s", "-C", _PKG_DIR], check=True)
+    return LIB_PATH
+
+
+def lib():
+    """Load the engine library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {_PKG_DIR}`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    sig = {
+        "smccat_version": ([], ctypes.c_char_p),
+        "smccat_last_error": ([], ctypes.c_char_p),
+        "smccat_discretize_gamma": ([ctypes.c_double, _i32, _dp], ctypes.c_int),
+        "smccat_lg_exchangeabilities": ([_dp], ctypes.c_int),
+        "smccat_create": ([ctypes.POINTER(Config), _up, ctypes.POINTER(vp)], ctypes.c_int),
+        "smccat_destroy": ([vp], ctypes.c_int),
+        "smccat_device_bytes": ([vp, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "smccat_set_particles": ([vp, _i32, _i32, _ip, _dp, _dp, _ip, _dp, _ip, _dp, _dp],
+                                 ctypes.c_int),
+        "smccat_get_particles": ([vp, _i32, _i32, _ip, _dp, _dp, _ip, _dp, _ip, _dp, _dp],
+                                 ctypes.c_int),
+        "smccat_refresh": ([vp, _i32, _i32, _i32], ctypes.c_int),
+        "smccat_get_lnl": ([vp, _i32, _i32, _dp], ctypes.c_int),
+        "smccat_get_site_lnl": ([vp, _i32, _dp], ctypes.c_int),
+        "smccat_set_branch_lengths": ([vp, _i32, _i32, _ip, _dp], ctypes.c_int),
+        "smccat_set_topology": ([vp, _i32, _ip, _dp], ctypes.c_int),
+        "smccat_set_pinv": ([vp, _i32, ctypes.c_double], ctypes.c_int),
+        "smccat_set_shape": ([vp, _i32, ctypes.c_double], ctypes.c_int),
+        "smccat_set_base": ([vp, _i32, _dp], ctypes.c_int),
+        "smccat_set_class_logits": ([vp, _i32, _i32, _dp], ctypes.c_int),
+        "smccat_accept": ([vp, _i32, _i32, _up], ctypes.c_int),
+        "smccat_sync": ([vp], ctypes.c_int),
+        "smccat_get_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
+        "smccat_set_profiling": ([vp, _i32], ctypes.c_int),
+        "smccat_get_profile": ([vp, ctypes.POINTER(Profile)], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise SmccatError(rc, lib().smccat_last_error().decode())
+
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(_ip)
+
+
+def version() -> str:
+    return lib().smccat_version().decode()
+
+
+def discretize_gamma(shape: float, num_rates: int) -> np.ndarray:
+    out = np.zeros(num_rates)
+    _check(lib().smccat_discretize_gamma(float(shape), int(num_rates), out.ctypes.data_as(_dp)))
+    return out
+
+
+def lg_exchangeabilities() -> np.ndarray:
+    out = np.zeros(190)
+    _check(lib().smccat_lg_exchangeabilities(out.ctypes.data_as(_dp)))
+    return out
+
+
+class Engine:
+    """One device context over a fixed alignment and a batch of particles.
+
+    Mirrors the reference's per-particle likelihood interface
+    (``class Particle``, src/analysis/Particle.hpp:48-125) as batched calls.
+    """
+
+    def __init__(self, codes, num_rates: int, max_particles: int, max_classes: int = 1,
+                 lg: bool = False, invar: bool = False, cat: bool = False, device: int = 0):
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        self.T, self.S = codes.shape
+        self.R = int(num_rates)
+        self.N = 2 * self.T - 1
+        self.P = int(max_particles)
+        self.Kmax = int(max_classes)
+        flags = (MODEL_LG if lg else 0) | (MODEL_INVAR if invar else 0) | (MODEL_CAT if cat else 0)
+        cfg = Config(self.T, self.S, self.R, self.P, self.Kmax, flags, PREC_FP64, device)
+        h = ctypes.c_void_p()
+        _check(lib().smccat_create(ctypes.byref(cfg), codes.ctypes.data_as(_up), ctypes.byref(h)))
+        self._h = h
+        self._codes = codes
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().smccat_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        v = ctypes.c_uint64(0)
+        _check(lib().smccat_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    # -- particle state ---------------------------------------------------
+    def set_particles(self, first, parent, branch, base, num_classes, logits, assign, pinv, shape):
+        par, pp = _i(parent)
+        n = par.shape[0]
+        br, bp = _d(branch)
+        ba, bap = _d(base)
+        nk, nkp = _i(num_classes)
+        lg = np.zeros((n, self.Kmax, 20))
+        lgs = np.asarray(logits, dtype=np.float64).reshape(n, -1, 20)
+        lg[:, :lgs.shape[1], :] = lgs
+        lg, lgp = _d(lg)
+        asg, ap = _i(assign)
+        pv, pvp = _d(pinv)
+        sh, shp = _d(shape)
+        _check(lib().smccat_set_particles(self._h, int(first), n, pp, bp, bap, nkp, lgp, ap, pvp, shp))
+
+    def get_particles(self, first=0, count=None):
+        count = self.P - first if count is None else count
+        out = dict(parent=np.zeros((count, self.N), np.int32), branch=np.zeros((count, self.N)),
+                   base=np.zeros((count, 190)), num_classes=np.zeros(count, np.int32),
+                   logits=np.zeros((count, self.Kmax, 20)),
+                   assign=np.zeros((count, self.S), np.int32), pinv=np.zeros(count),
+                   shape=np.zeros(count))
+        _check(lib().smccat_get_particles(
+            self._h, int(first), int(count), out["parent"].ctypes.data_as(_ip),
+            out["branch"].ctypes.data_as(_dp), out["base"].ctypes.data_as(_dp),
+            out["num_classes"].ctypes.data_as(_ip), out["logits"].ctypes.data_as(_dp),
+            out["assign"].ctypes.data_as(_ip), out["pinv"].ctypes.data_as(_dp),
+            out["shape"].ctypes.data_as(_dp)))
+        return out
+
+    def refresh(self, first=0, count=None, full=False):
+        count = self.P - first if count is None else count
+        _check(lib().smccat_refresh(self._h, int(first), int(count),
+                                    REFRESH_FULL if full else REFRESH_DIRTY))
+
+    def lnl(self, first=0, count=None) -> np.ndarray:
+        count = self.P - first if count is None else count
+        out = np.zeros(count)
+        _check(lib().smccat_get_lnl(self._h, int(first), int(count), out.ctypes.data_as(_dp)))
+        return out
+
+    def site_lnl(self, p) -> np.ndarray:
+        out = np.zeros(self.S)
+        _check(lib().smccat_get_site_lnl(self._h, int(p), out.ctypes.data_as(_dp)))
+        return out
+
+    # -- edits --------------------------------------------------------------
+    def set_branch_lengths(self, p, nodes, lengths):
+        nd, ndp = _i(nodes)
+        ln, lnp = _d(lengths)
+        _check(lib().smccat_set_branch_lengths(self._h, int(p), len(nd), ndp, lnp))
+
+    def set_topology(self, p, parent, branch):
+        par, pp = _i(parent)
+        br, bp = _d(branch)
+        _check(lib().smccat_set_topology(self._h, int(p), pp, bp))
+
+    def set_pinv(self, p, v):
+        _check(lib().smccat_set_pinv(self._h, int(p), float(v)))
+
+    def set_shape(self, p, v):
+        _check(lib().smccat_set_shape(self._h, int(p), float(v)))
+
+    def set_base(self, p, base):
+        b, bp = _d(base)
+        _check(lib().smccat_set_base(self._h, int(p), bp))
+
+    def set_class_logits(self, p, k, logits):
+        lg, lgp = _d(logits)
+        _check(lib().smccat_set_class_logits(self._h, int(p), int(k), lgp))
+
+    def accept(self, mask, first=0):
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        _check(lib().smccat_accept(self._h, int(first), len(m), m.ctypes.data_as(_up)))
+
+    def sync(self):
+        _check(lib().smccat_sync(self._h))
+
+    # -- measurement --------------------------------------------------------
+    @property
+    def stream_ptr(self) -> int:
+        """The cudaStream_t the engine launches on (for caller-side events)."""
+        v = ctypes.c_void_p()
+        _check(lib().smccat_get_stream(self._h, ctypes.byref(v)))
+        return v.value or 0
+
+    def set_profiling(self, enable: bool):
+        _check(lib().smccat_set_profiling(self._h, 1 if enable else 0))
+
+    def profile(self) -> dict:
+        pr = Profile()
+        _check(lib().smccat_get_profile(self._h, ctypes.byref(pr)))
+        return dict(launches={n: int(pr.launches[i]) for i, n in enumerate(KERNEL_NAMES)},
+                    ms={n: float(pr.ms[i]) for i, n in enumerate(KERNEL_NAMES)},
+                    h2d_bytes=int(pr.h2d_bytes), d2h_bytes=int(pr.d2h_bytes))
