@@ -131,6 +131,14 @@ int smccat_get_lnl(smccat_ctx* ctx, int32_t first, int32_t count, double* out);
  * The reference keeps no per-site output; this is the parity probe. */
 int smccat_get_site_lnl(smccat_ctx* ctx, int32_t p, double* out);
 
+/* Transition matrix P(t r) of particle p, class k, the edge above `node`
+ * and rate category r, as 400 row-major doubles (P[i][j] = Pr(j | i)), from
+ * the current state after its last refresh. Parity probe for
+ * TransitionProbabilityClass::transitionProbabilities
+ * (TransitionProbabilityClass.hpp:25, filled at .cpp:83-95). */
+int smccat_get_transition_matrix(smccat_ctx* ctx, int32_t p, int32_t k, int32_t node,
+                                 int32_t r, double* out400);
+
 /* ---- edits that mark dirty state (the proposal side of the moves) ------ */
 
 /* Set branch lengths of `n` nodes of particle p. Marks the transition

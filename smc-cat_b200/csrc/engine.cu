@@ -35,6 +35,12 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+}  // namespace
+
+void smccat::set_last_error(const std::string& msg) { g_err = msg; }
+
+namespace {
+
 #define CK(call)                                                                      \
     do {                                                                              \
         cudaError_t e_ = (call);                                                      \
@@ -700,6 +706,27 @@ int smccat_get_site_lnl(smccat_ctx* c, int32_t p, double* out) {
     CK(cudaSetDevice(c->cfg.device));
     CK(d2h(c, out, c->d_site_lnl + (size_t)p * c->d.S, c->d.S * sizeof(double)));
     CK(cudaStreamSynchronize(c->st));
+    return SMCCAT_OK;
+}
+
+int smccat_get_transition_matrix(smccat_ctx* c, int32_t p, int32_t k, int32_t node, int32_t r,
+                                 double* out400) {
+    int rc = check_particle(c, p);
+    if (rc) return rc;
+    const Slot& s = c->slots[p];
+    const Dims& d = c->d;
+    if (!out400 || k < 0 || k >= s.cur.K || node < 0 || node >= d.N || node == s.cur.root ||
+        r < 0 || r >= d.R)
+        return fail(SMCCAT_EINVAL, "bad class / node / rate index");
+    if (s.pending && !s.refreshed) return fail(SMCCAT_ESTATE, "particle has unrefreshed edits");
+    double blk[kPBlock];
+    const size_t off = ((((size_t)p * d.Kmax + k) * d.N + node) * 2 + s.cur.pws[node]) *
+                           (size_t)d.R * kPBlock + (size_t)r * kPBlock;
+    CK(cudaSetDevice(c->cfg.device));
+    CK(d2h(c, blk, c->d_Pm + off, sizeof(blk)));
+    CK(cudaStreamSynchronize(c->st));
+    for (int i = 0; i < kStates; ++i)
+        for (int j = 0; j < kStates; ++j) out400[i * kStates + j] = blk[j * kStates + i];
     return SMCCAT_OK;
 }
 

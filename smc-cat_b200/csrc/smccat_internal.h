@@ -18,7 +18,12 @@
 #pragma once
 #include <stdint.h>
 
+#include <string>
+
 namespace smccat {
+
+// Record the message smccat_last_error() returns on this thread.
+void set_last_error(const std::string& msg);
 
 constexpr int kStates = 20;
 constexpr int kBase = 190;

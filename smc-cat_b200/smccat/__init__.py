@@ -81,6 +81,7 @@ def lib():
         "smccat_refresh": ([vp, _i32, _i32, _i32], ctypes.c_int),
         "smccat_get_lnl": ([vp, _i32, _i32, _dp], ctypes.c_int),
         "smccat_get_site_lnl": ([vp, _i32, _dp], ctypes.c_int),
+        "smccat_get_transition_matrix": ([vp, _i32, _i32, _i32, _i32, _dp], ctypes.c_int),
         "smccat_set_branch_lengths": ([vp, _i32, _i32, _ip, _dp], ctypes.c_int),
         "smccat_set_topology": ([vp, _i32, _ip, _dp], ctypes.c_int),
         "smccat_set_pinv": ([vp, _i32, ctypes.c_double], ctypes.c_int),
@@ -223,6 +224,13 @@ class Engine:
     def site_lnl(self, p) -> np.ndarray:
         out = np.zeros(self.S)
         _check(lib().smccat_get_site_lnl(self._h, int(p), out.ctypes.data_as(_dp)))
+        return out
+
+    def transition_matrix(self, p, k, node, r) -> np.ndarray:
+        """P(t r) (row-major 20x20) of particle p, class k, edge above node."""
+        out = np.zeros((20, 20))
+        _check(lib().smccat_get_transition_matrix(self._h, int(p), int(k), int(node), int(r),
+                                                  out.ctypes.data_as(_dp)))
         return out
 
     # -- edits --------------------------------------------------------------

@@ -81,6 +81,27 @@ def test_golden_cases(case):
     eng.close()
 
 
+def test_transition_matrices_match_oracle():
+    """Device spectral decomposition + P(t r) against the oracle, every edge."""
+    cfg = SMALL[2]
+    eng, codes, st = make_engine(cfg, 2, 31)
+    worst = 0.0
+    for p in range(2):
+        rates = oracle.discretize_gamma(st["shape"][p], cfg.R)
+        root = int(np.where(st["parent"][p] < 0)[0][0])
+        for k in range(int(st["num_classes"][p])):
+            pi = oracle.softmax20(st["logits"][p, k])
+            for node in range(2 * cfg.T - 1):
+                if node == root:
+                    continue
+                for r in range(cfg.R):
+                    ref = oracle.transition(st["base"][p], pi, st["branch"][p, node] * rates[r])
+                    got = eng.transition_matrix(p, k, node, r)
+                    worst = max(worst, np.abs(got - ref).max())
+    assert worst < 1e-13
+    eng.close()
+
+
 def _nni(parent, rng):
     """Swap a child of an internal non-root node p with its sibling's side."""
     parent = parent.copy()
