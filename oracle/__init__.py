@@ -6,8 +6,9 @@ reference citations). Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU
 baseline leg of ``bench.py`` may import this module, and only as a checker or as
 the timed CPU baseline -- never as part of the product path.
 
-Parity status: the reference (C++23 on Eigen + Boost) cannot be compiled on
-this machine. The oracle is pinned against golden vectors produced by
+Parity status: parity unpinned. The reference (C++23 on Eigen + Boost) has no
+tests or golden vectors and cannot be compiled on this machine. The oracle is
+checked instead against golden vectors produced by
 ``tests/golden/make_golden.py``, an independent numpy/scipy restatement that
 follows the reference's own formulas (general eigendecomposition + inverse for
 P(t), Boost-equivalent gamma quantiles) and parses the LG table out of the

@@ -5,9 +5,10 @@
 // checker, and by bench.py as the timed CPU baseline (the reference's own
 // OpenMP-over-particles structure). Nothing in the product links or calls it.
 //
-// Parity status: the reference itself cannot be compiled on this machine (its
-// arithmetic lives in Eigen >= 3.4 and Boost.Math, neither installed), so this
-// restatement is pinned against golden vectors produced by an independent
+// Parity status: parity unpinned. The reference ships no tests or golden
+// vectors, and it cannot be compiled on this machine (its arithmetic lives in
+// Eigen >= 3.4 and Boost.Math, neither installed), so this restatement is
+// checked instead against golden vectors produced by an independent
 // numpy/scipy restatement (tests/golden/make_golden.py) that follows the
 // reference's own formulas -- general complex eigendecomposition + inverse for
 // P(t) (Eigen::EigenSolver's role, here LAPACK dgeev) and the gamma quantile
