@@ -82,6 +82,29 @@ int smccat_discretize_gamma(double shape, int32_t num_rates, double* out);
  * (Particle.cpp:84-94). Host-only. */
 int smccat_lg_exchangeabilities(double* out190);
 
+/* Batched transition matrices for callers that cannot allocate device memory.
+ * No counterpart in the reference. Some hosts of this library may not call
+ * cudaMalloc at all -- code living inside another framework's memory budget or
+ * custom allocator, or a plugin that is only handed pre-allocated buffers --
+ * so this entry point allocates nothing: the caller passes device buffers for
+ * every input and output, and the intermediate spectral data go to a
+ * fixed-size array compiled into the library (3.5 MB, kept on every GPU that
+ * loads the library's kernels until the process exits).
+ *   base    [num_classes][190]  log-exchangeabilities (device)
+ *   logits  [num_classes][20]   stationary logits (device)
+ *   times   [num_classes][num_times]  branch length x rate (device)
+ *   p_out   [num_classes][num_times][20][20]  row-major P(t) (device)
+ * num_classes may be at most 512; larger requests return SMCCAT_EINVAL. Work
+ * is queued on `stream` (a cudaStream_t, NULL = legacy default stream) on the
+ * current device and the call returns without waiting. The first call on a
+ * device resolves the array's device address (one-time set-up, done with that
+ * device current); make that first call before any stream capture. Every call
+ * reuses the same array, so calls whose work overlaps on the GPU (e.g. on two
+ * streams at once) race; order them on one stream. */
+int smccat_transition_matrices_noalloc(int32_t num_classes, const double* base,
+                                       const double* logits, int32_t num_times,
+                                       const double* times, double* p_out, void* stream);
+
 /* Create a context over the alignment `codes` [T][S] (row-major, taxon-major).
  * Replaces the data half of Particle::Particle (Particle.cpp:21-73): tip
  * encoding and the invariant-site flags are derived once and shared by all

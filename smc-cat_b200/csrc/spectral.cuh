@@ -14,14 +14,14 @@
 
 namespace smccat {
 
-__device__ __forceinline__ double warp_sum(double v) {
+static __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
 
 // Run by exactly one full warp; `rec` holds kSpecStride doubles.
-__device__ __noinline__ void spectral_decompose_warp(const double* __restrict__ base,
+static __device__ __noinline__ void spectral_decompose_warp(const double* __restrict__ base,
                                                      const double* __restrict__ logits,
                                                      double* __restrict__ rec) {
     const int lane = threadIdx.x;
