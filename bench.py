@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=32,
                     help="particles per CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--particles", type=int, default=0,
+                    help="override the particle count (small cases for ncu captures)")
+    ap.add_argument("--skip-e2e", action="store_true")
     return ap.parse_args()
 
 
@@ -248,8 +251,8 @@ def main():
     rng = np.random.default_rng(cfg.seed)
     codes, _ = workload.simulate_alignment(cfg, rng)
     prng = np.random.default_rng(cfg.seed * 1000 + rank)
-    st = workload.make_particles(cfg, cfg.particles, prng)
-    n = cfg.particles
+    n = args.particles or cfg.particles
+    st = workload.make_particles(cfg, n, prng)
     eng = smccat.Engine(codes, cfg.R, n, max_classes=st["logits"].shape[1], lg=cfg.lg,
                         invar=cfg.invar, cat=cfg.cat, device=local)
     load = lambda: eng.set_particles(0, st["parent"], st["branch"], st["base"],  # noqa: E731
@@ -257,6 +260,7 @@ def main():
                                      st["shape"])
     load()
     eng.refresh(full=True)
+    tuned = eng.autotune(reps=2)
     stream = torch.cuda.ExternalStream(eng.stream_ptr, device=torch.device("cuda", local))
     units_per_step = n * cfg.S * cfg.R
 
@@ -281,9 +285,9 @@ def main():
     eng.set_profiling(False)
 
     # ---- e2e through the C-ABI with host buffers ----------------------------
-    lnl_host = None
+    lnl_host = eng.lnl()
     eng.set_profiling(False)
-    for _ in range(2):
+    for _ in range(0 if args.skip_e2e else 2):
         load()
         eng.refresh(full=True)
         lnl_host = eng.lnl()
@@ -292,7 +296,7 @@ def main():
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     f0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(0 if args.skip_e2e else args.steps):
         load()
         eng.refresh(full=True)
         lnl_host = eng.lnl()
@@ -309,7 +313,7 @@ def main():
     ms, ms_e2e = times.tolist()
     total_units = units_per_step * args.steps * world
     value = total_units / (ms * 1e-3)
-    e2e_value = total_units / (ms_e2e * 1e-3)
+    e2e_value = None if args.skip_e2e else total_units / (ms_e2e * 1e-3)
 
     if rank == 0:
         b_unit, f_unit = algorithmic_cost(cfg.T, cfg.R)
@@ -338,7 +342,8 @@ def main():
                        "particles_per_gpu": n, "model": "GTR+G4+I" if args.config == 2 else cfg.name,
                        "step": "full refresh of every particle (refreshLikelihood(true))",
                        "l2": "inputs larger than L2 (CL buffers %.1f GB per GPU)" % (eng.device_bytes / 1e9),
-                       "parallelism": f"particles sharded, {world} GPU(s), no collective"},
+                       "parallelism": f"particles sharded, {world} GPU(s), no collective",
+                       "autotune": tuned},
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": prof_e2e["h2d_bytes"] // args.steps,
                     "d2h_bytes_per_step": prof_e2e["d2h_bytes"] // args.steps},

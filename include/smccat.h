@@ -39,6 +39,7 @@ extern "C" {
 #define SMCCAT_ESTATE    4  /* call out of protocol order                   */
 #define SMCCAT_ENUMERIC  5  /* a likelihood came out NaN                     */
 #define SMCCAT_ENODEV    6  /* no usable CUDA device                         */
+#define SMCCAT_ETIMEOUT  7  /* a bounded device-side wait gave up            */
 
 /* model_flags */
 #define SMCCAT_MODEL_LG     1  /* LG exchangeabilities (else GTR, inferred)  */
@@ -223,6 +224,13 @@ typedef struct smccat_profile {
     uint64_t h2d_bytes;                     /* host->device bytes copied        */
     uint64_t d2h_bytes;                     /* device->host bytes copied        */
 } smccat_profile;
+
+/* Time every instantiated pruning-kernel variant (register caps / CTAs per
+ * SM) with `reps` full refreshes of the loaded particles [0, n) and keep the
+ * fastest for this context. Writes the chosen variant and, if ms_out is not
+ * NULL, the per-variant pruning time (ms) for each variant (at most 8). The
+ * particles must have no pending edits; their likelihoods are recomputed. */
+int smccat_autotune(smccat_ctx* ctx, int32_t reps, int32_t* variant_out, double* ms_out);
 
 /* Enable (1) or disable (0) per-launch CUDA-event timing; resets counters. */
 int smccat_set_profiling(smccat_ctx* ctx, int32_t enable);

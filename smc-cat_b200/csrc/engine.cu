@@ -105,6 +105,7 @@ struct smccat_ctx {
     uint8_t* h_sws = nullptr;   // pinned mirror of d_sws
     size_t plan_cap = 0;
     int tile_cap = 0;
+    int prune_variant = 0;      // chosen by smccat_autotune
 
     std::vector<uint8_t> codes;
     std::vector<Slot> slots;
@@ -651,9 +652,11 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
     a.LSC = c->d_LSC;
     a.site_lnl = c->d_site_lnl;
     a.partial = c->d_partial;
+    a.status = c->d_status;
     const int ntiles = c->tile_off[first + count] - c->tile_off[first];
     if (ntiles > 0)
-        CK(launch(c, SMCCAT_KERNEL_PRUNE, [&] { return launch_prune(a, ntiles, c->st); }));
+        CK(launch(c, SMCCAT_KERNEL_PRUNE,
+                  [&] { return launch_prune(a, ntiles, c->prune_variant, c->st); }));
     CK(launch(c, SMCCAT_KERNEL_REDUCE, [&] {
         return launch_reduce(c->d_tile_off, c->d_partial, d_hdr, first, count, c->d_lnl, c->d_status, c->st);
     }));
@@ -684,6 +687,8 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
     CK(cudaStreamSynchronize(c->st));
     if (status) {
         CK(cudaMemset(c->d_status, 0, sizeof(int)));
+        if (status & 2)
+            return fail(SMCCAT_ETIMEOUT, "a pruning warp gave up waiting for its transition matrices");
         return fail(SMCCAT_ENUMERIC, "a log-likelihood came out NaN");
     }
     return SMCCAT_OK;
@@ -726,7 +731,7 @@ int smccat_get_transition_matrix(smccat_ctx* c, int32_t p, int32_t k, int32_t no
     CK(d2h(c, blk, c->d_Pm + off, sizeof(blk)));
     CK(cudaStreamSynchronize(c->st));
     for (int i = 0; i < kStates; ++i)
-        for (int j = 0; j < kStates; ++j) out400[i * kStates + j] = blk[j * kStates + i];
+        for (int j = 0; j < kStates; ++j) out400[i * kStates + j] = blk[i * kPCols + j];
     return SMCCAT_OK;
 }
 
@@ -860,6 +865,47 @@ int smccat_accept(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* ma
         s.pending = false;
         s.refreshed = false;
     }
+    return SMCCAT_OK;
+}
+
+int smccat_autotune(smccat_ctx* c, int32_t reps, int32_t* variant_out, double* ms_out) {
+    if (!c) return fail(SMCCAT_EINVAL, "null context");
+    int n = 0;
+    while (n < c->cfg.max_particles && c->slots[n].loaded) ++n;
+    if (n == 0) return fail(SMCCAT_ESTATE, "autotune needs loaded particles");
+    for (int i = 0; i < n; ++i)
+        if (c->slots[i].pending && !c->slots[i].commit_on_refresh)
+            return fail(SMCCAT_ESTATE, "autotune needs particles without pending edits");
+    reps = std::max(1, reps);
+    const bool timing = c->timing;
+    const smccat_profile saved = c->prof;
+    const int nv = prune_variants(c->d.R);
+    int best = 0;
+    double best_ms = INFINITY;
+    for (int v = 0; v < nv; ++v) {
+        c->prune_variant = v;
+        int rc = smccat_refresh(c, 0, n, SMCCAT_REFRESH_FULL);  // warm-up, also commits loads
+        if (rc) return rc;
+        c->timing = true;
+        c->ev_used.clear();
+        c->prof = smccat_profile{};
+        for (int k = 0; k < reps; ++k) {
+            rc = smccat_refresh(c, 0, n, SMCCAT_REFRESH_FULL);
+            if (rc) return rc;
+        }
+        smccat_profile pr;
+        rc = smccat_get_profile(c, &pr);
+        if (rc) return rc;
+        const double ms = pr.ms[SMCCAT_KERNEL_PRUNE] / reps;
+        if (ms_out) ms_out[v] = ms;
+        if (ms < best_ms) { best_ms = ms; best = v; }
+        c->timing = false;
+    }
+    c->prune_variant = best;
+    c->timing = timing;
+    c->ev_used.clear();
+    c->prof = saved;
+    if (variant_out) *variant_out = best;
     return SMCCAT_OK;
 }
 

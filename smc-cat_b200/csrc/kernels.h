@@ -28,12 +28,15 @@ struct PruneArgs {
     double* LSC;
     double* site_lnl;
     double* partial;
+    int* status;      // bit 1: NaN likelihood, bit 2: a bounded wait gave up
 };
 
 cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d, cudaStream_t st);
 cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, const uint8_t* sws,
                         const double* spec, double* Pm, const Dims& d, cudaStream_t st);
-cudaError_t launch_prune(const PruneArgs& a, int ntiles, cudaStream_t st);
+// Pruning kernel variants (register caps) available for R rate categories.
+int prune_variants(int R);
+cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
 cudaError_t launch_reduce(const int32_t* tile_off, const double* partial, const PartHdr* hdr, int first,
                           int count, double* lnl, int* status, cudaStream_t st);
 cudaError_t launch_accept(double* lnl, double* lnl_old, const uint8_t* mask, int first, int count,

@@ -1,19 +1,21 @@
 // FP64 kernels of the B200 likelihood engine.
 //
-//   spec_kernel   one warp per (particle, class): softmax of the logits, the
-//                 normalised rate matrix Q (TransitionProbabilityClass.cpp:50-75),
-//                 and a parallel (round-robin) Jacobi eigendecomposition of the
-//                 symmetrised S = D^1/2 Q D^-1/2. Stores lambda, L = D^-1/2 U,
-//                 Rm = U^T D^1/2 and pi.
+//   spec_kernel   one warp per (particle, class): spectral decomposition of the
+//                 class's rate matrix (spectral.cuh).
 //   pmat_kernel   one CTA per (particle, node): P(t r) = L diag(exp(lambda t r)) Rm
 //                 for every class and rate (TransitionProbabilityClass.cpp:83-95),
-//                 stored transposed with a 21st row of row sums.
-//   prune_kernel  one CTA per (particle, tile of <= 64 same-class sites): walks the
-//                 particle's dirty internal nodes in post-order
-//                 (Particle.cpp:577-626), child CLs streamed from HBM, P staged in
-//                 shared memory, per-(site, rate) power-of-two rescaling, then the
-//                 root reduction of the tile (Particle.cpp:634-674) with a
-//                 shared-memory log-sum-exp over rates and a warp-shuffle sum.
+//                 row-major with a row-sum column.
+//   prune_kernel  one warp per (rate, tile of <= 32 same-class sites), R warps per
+//                 CTA: walks the particle's dirty internal nodes in post-order
+//                 (Particle.cpp:577-626). Each warp stages its two children's P
+//                 blocks into shared memory with TMA bulk copies (double-buffered,
+//                 mbarrier-tracked, the next node's copy in flight while the
+//                 current node computes), keeps the partial it just produced in
+//                 registers (in a post-order of an upward-closed dirty set the
+//                 previous node is always a child of the next one), reads at most
+//                 one child partial back from memory, rescales each (site, rate)
+//                 by an exact power of two, then the CTA reduces the root
+//                 (Particle.cpp:634-674): log-sum-exp over rates, +I, warp sum.
 //   reduce_kernel per particle, sums the tile partials in a fixed order.
 #include <cuda_runtime.h>
 #include <math.h>
@@ -23,6 +25,79 @@
 
 namespace smccat {
 
+namespace {
+
+constexpr uint32_t kWaitLimit = 1u << 22;  // mbarrier polls before giving up
+constexpr uint32_t kPBytes = kPBlock * sizeof(double);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// Bulk (non-tensor) TMA copy global -> shared, completion counted on `bar`.
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `parity` of `bar` to complete; false after kWaitLimit polls.
+__device__ __noinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// acc[i] = sum_j P[i][j] x[j] with P row-major (stride kPCols), broadcast reads.
+__device__ __forceinline__ void matvec(const double* __restrict__ P, const double* x, double* acc) {
+#pragma unroll
+    for (int i = 0; i < kStates; ++i) {
+        const double2* row = reinterpret_cast<const double2*>(P + i * kPCols);
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int j = 0; j < kStates / 2; ++j) {
+            const double2 p2 = row[j];
+            s0 = fma(p2.x, x[2 * j], s0);
+            s1 = fma(p2.y, x[2 * j + 1], s1);
+        }
+        acc[i] = s0 + s1;
+    }
+}
+
+}  // namespace
 
 // ---------------------------------------------------------------------------
 // Spectral decomposition of one class (one warp).
@@ -70,12 +145,12 @@ __global__ void __launch_bounds__(128) pmat_kernel(const PJob* __restrict__ jobs
                                (size_t)d.R * kPBlock;
         for (int idx = tid; idx < d.R * kPBlock; idx += blockDim.x) {
             const int r = idx / kPBlock, e = idx % kPBlock;
-            const int row = e / kStates, i = e % kStates;
+            const int i = e / kPCols, j = e % kPCols;
             double v = 0.0;
-            if (row < kStates) {
+            if (j < kStates) {
 #pragma unroll
-                for (int m = 0; m < kStates; ++m) v = fma(L[i][m] * ex[r][m], Rm[m][row], v);
-            } else {
+                for (int m = 0; m < kStates; ++m) v = fma(L[i][m] * ex[r][m], Rm[m][j], v);
+            } else if (j == kStates) {
 #pragma unroll
                 for (int m = 0; m < kStates; ++m) v = fma(L[i][m] * ex[r][m], rs[m], v);
             }
@@ -85,110 +160,188 @@ __global__ void __launch_bounds__(128) pmat_kernel(const PJob* __restrict__ jobs
 }
 
 // ---------------------------------------------------------------------------
-// Pruning + root reduction of one tile.
-template <int R>
-__device__ __forceinline__ void child_vector(const PruneArgs& a, const double* __restrict__ Pt,
-                                             int child, int wsc, const double* CLp,
-                                             size_t node_stride, size_t ws_stride,
-                                             size_t j_stride, int col, int site, double* v) {
-    if (child < a.d.T) {
-        const int code = a.codes[(size_t)child * a.d.S + site];
-        const int row = code < kStates ? code : kStates;
-#pragma unroll
-        for (int i = 0; i < kStates; ++i) v[i] = Pt[row * kStates + i];
-    } else {
-        const double* x = CLp + (size_t)(child - a.d.T) * node_stride + wsc * ws_stride + col;
-#pragma unroll
-        for (int i = 0; i < kStates; ++i) v[i] = 0.0;
-#pragma unroll
-        for (int j = 0; j < kStates; ++j) {
-            // Plain load: the child may have been written earlier in this
-            // kernel by this same thread, so the read-only path is not safe.
-            const double xj = x[j * j_stride];
-#pragma unroll
-            for (int i = 0; i < kStates; ++i) v[i] = fma(Pt[j * kStates + i], xj, v[i]);
-        }
-    }
-}
-
-template <int R>
-__global__ void __launch_bounds__(kTileSites * R, (R <= 4 ? 2 : 1)) prune_kernel(const PruneArgs a) {
+// Pruning + root reduction of one tile: warp r handles rate category r.
+// MINB = CTAs per SM the register allocation must allow (the register cap is
+// 65536 / (32 R MINB)); the autotuner picks among the instantiated values.
+template <int R, int MINB>
+__global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) {
     const Dims d = a.d;
     const int tile_id = a.tile_begin + blockIdx.x;
     const Tile tl = a.tiles[tile_id];
     const int p = tl.p;
     const PartHdr* h = a.hdr + (p - a.first);
     if (!h->active) return;  // uniform across the CTA
-    const int tid = threadIdx.x;
-    const int r = tid / kTileSites, sl = tid % kTileSites;
-    const bool valid = sl < tl.nslots;
-    const int slot = tl.slot0 + (valid ? sl : 0);
-    const int site = a.perm[(size_t)p * d.S + slot];
 
-    extern __shared__ __align__(16) double sP[];  // [2 children][R][21][20]
-    __shared__ double red[R][kTileSites];
-    __shared__ double wsum[2];
+    extern __shared__ __align__(128) double smem[];  // [R warps][2 buffers][2 children][kPBlock]
+    __shared__ __align__(8) uint64_t bars[R][2];
+    __shared__ double red[R][32];
+    __shared__ int bad;
+
+    const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
+    const bool valid = lane < tl.nslots;
+    const int slot = tl.slot0 + (valid ? lane : 0);
+    const int site = a.perm[(size_t)p * d.S + slot];
+    double* buf = smem + (size_t)r * 4 * kPBlock;
 
     const size_t j_stride = (size_t)R * d.Spad;
     const size_t ws_stride = (size_t)kStates * j_stride;
     const size_t node_stride = 2 * ws_stride;
-    const size_t lws_stride = (size_t)R * d.Spad;
-    const double* CLp = a.CL + (size_t)p * d.NI * node_stride;
-    double* CLw = a.CL + (size_t)p * d.NI * node_stride;
+    const size_t lws_stride = j_stride;
+    double* CLp = a.CL + (size_t)p * d.NI * node_stride;
     double* LSCp = a.LSC + (size_t)p * d.NI * 2 * lws_stride;
     const int col = r * d.Spad + slot;
+    const double* Pcls = a.Pm + ((size_t)p * d.Kmax + tl.k) * d.N * 2 * (size_t)R * kPBlock +
+                         (size_t)r * kPBlock;
+    auto pblock = [&](int child, int pws) {
+        return Pcls + ((size_t)child * 2 + pws) * (size_t)R * kPBlock;
+    };
+
+    if (threadIdx.x == 0) bad = 0;
+    if (lane == 0) {
+        mbar_init(&bars[r][0], 1);
+        mbar_init(&bars[r][1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    const int cnt = h->node_cnt;
+    const NodeJob* nodes = a.nodes + h->node_off;
+    if (cnt > 0 && lane == 0) {
+        const NodeJob nj = nodes[0];
+        mbar_expect_tx(&bars[r][0], 2 * kPBytes);
+        tma_load_1d(buf, pblock(nj.c1, (nj.ws >> 3) & 1), kPBytes, &bars[r][0]);
+        tma_load_1d(buf + kPBlock, pblock(nj.c2, (nj.ws >> 4) & 1), kPBytes, &bars[r][0]);
+    }
 
     double y[kStates];
     double lsc = 0.0;
-    const int cnt = h->node_cnt;
+    int prev = -1;
+    bool ok = true;
+    uint32_t phase = 0;
     for (int q = 0; q < cnt; ++q) {
-        const NodeJob nj = a.nodes[h->node_off + q];
-        __syncthreads();
-        for (int idx = tid; idx < 2 * R * kPBlock; idx += blockDim.x) {
-            const int c = idx / (R * kPBlock);
-            const int rem = idx - c * R * kPBlock;
-            const int child = c ? nj.c2 : nj.c1;
-            const int pws = (nj.ws >> (3 + c)) & 1;
-            sP[idx] = a.Pm[((((size_t)p * d.Kmax + tl.k) * d.N + child) * 2 + pws) * (size_t)R * kPBlock + rem];
+        const int b = q & 1;
+        const NodeJob nj = nodes[q];
+        if (q + 1 < cnt && lane == 0) {
+            // Buffer b^1 was last read at node q-1 (the warp synchronised after it).
+            const NodeJob nx = nodes[q + 1];
+            fence_proxy_async();
+            mbar_expect_tx(&bars[r][b ^ 1], 2 * kPBytes);
+            tma_load_1d(buf + (b ^ 1) * 2 * kPBlock, pblock(nx.c1, (nx.ws >> 3) & 1), kPBytes,
+                        &bars[r][b ^ 1]);
+            tma_load_1d(buf + (b ^ 1) * 2 * kPBlock + kPBlock, pblock(nx.c2, (nx.ws >> 4) & 1),
+                        kPBytes, &bars[r][b ^ 1]);
         }
-        __syncthreads();
+        // Roles: the child computed just before (if any) is in registers; the
+        // other child is a tip (gather) or a stored partial (load).
+        const bool c1prev = nj.c1 == prev, c2prev = nj.c2 == prev;
+        const int oi = c1prev ? 1 : 0;  // index of the "other" child (c1 when neither is prev)
+        const int o = oi ? nj.c2 : nj.c1;
+        const int fi = 1 - oi;          // index of the register / first child
+        double lsc_o = 0.0;
+        int code_o = 0;
         if (valid) {
-            const int ws1 = (nj.ws >> 1) & 1, ws2 = (nj.ws >> 2) & 1, wso = nj.ws & 1;
-            child_vector<R>(a, sP + r * kPBlock, nj.c1, ws1, CLp, node_stride, ws_stride,
-                            j_stride, col, site, y);
-            double v2[kStates];
-            child_vector<R>(a, sP + (R + r) * kPBlock, nj.c2, ws2, CLp, node_stride, ws_stride,
-                            j_stride, col, site, v2);
+            if (o >= d.T) {
+                const int wsc = (nj.ws >> (1 + oi)) & 1;
+                lsc_o = LSCp[(size_t)(o - d.T) * 2 * lws_stride + wsc * lws_stride + col];
+            } else {
+                code_o = a.codes[(size_t)o * d.S + site];
+            }
+        }
+        if (ok && !mbar_wait_bounded(&bars[r][b], (phase >> b) & 1)) {
+            ok = false;
+            atomicOr(a.status, 2);
+        }
+        phase ^= 1u << b;
+        if (ok && valid) {
+            const double* Pf = buf + (size_t)(b * 2 + fi) * kPBlock;
+            const double* Po = buf + (size_t)(b * 2 + oi) * kPBlock;
+            double acc[kStates];
+            double lsc_f = 0.0;
+            if (c1prev || c2prev) {
+                matvec(Pf, y, acc);
+                lsc_f = lsc;
+            } else {
+                // Neither child was just computed (both-tip nodes, or a list that
+                // is not a plain post-order): the first child comes from memory.
+                const int f = fi ? nj.c2 : nj.c1;
+                if (f >= d.T) {
+                    const int wsf = (nj.ws >> (1 + fi)) & 1;
+                    const double* fp = CLp + (size_t)(f - d.T) * node_stride + wsf * ws_stride + col;
+#pragma unroll
+                    for (int j = 0; j < kStates; ++j) y[j] = fp[j * j_stride];
+                    lsc_f = LSCp[(size_t)(f - d.T) * 2 * lws_stride + wsf * lws_stride + col];
+                    matvec(Pf, y, acc);
+                } else {
+                    const int code = a.codes[(size_t)f * d.S + site];
+                    const int cc = code < kStates ? code : kStates;
+#pragma unroll
+                    for (int i = 0; i < kStates; ++i) acc[i] = Pf[i * kPCols + cc];
+                }
+            }
+            if (o >= d.T) {
+                // The register child is consumed; its registers now hold the
+                // other child's stored partial, folded in row by row.
+                const int wsc = (nj.ws >> (1 + oi)) & 1;
+                const double* xp = CLp + (size_t)(o - d.T) * node_stride + wsc * ws_stride + col;
+#pragma unroll
+                for (int j = 0; j < kStates; ++j) y[j] = xp[j * j_stride];
+#pragma unroll
+                for (int i = 0; i < kStates; ++i) {
+                    const double2* row = reinterpret_cast<const double2*>(Po + i * kPCols);
+                    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                    for (int j = 0; j < kStates / 2; ++j) {
+                        const double2 p2 = row[j];
+                        s0 = fma(p2.x, y[2 * j], s0);
+                        s1 = fma(p2.y, y[2 * j + 1], s1);
+                    }
+                    acc[i] *= s0 + s1;
+                }
+            } else {
+                const int cc = code_o < kStates ? code_o : kStates;
+#pragma unroll
+                for (int i = 0; i < kStates; ++i) acc[i] *= Po[i * kPCols + cc];
+            }
             double mx = 0.0;
 #pragma unroll
-            for (int i = 0; i < kStates; ++i) { y[i] *= v2[i]; mx = fmax(mx, y[i]); }
-            double l = 0.0;
+            for (int i = 0; i < kStates; ++i) mx = fmax(mx, acc[i]);
+            double l;
             if (mx > 0.0) {
                 int e;
                 frexp(mx, &e);
                 const double sc = ldexp(1.0, -e);
 #pragma unroll
-                for (int i = 0; i < kStates; ++i) y[i] *= sc;
+                for (int i = 0; i < kStates; ++i) acc[i] *= sc;
                 l = e * 0.69314718055994530942;
             } else {
                 l = (mx == 0.0) ? -INFINITY : NAN;
             }
-            if (nj.c1 >= d.T)
-                l += LSCp[(size_t)(nj.c1 - d.T) * 2 * lws_stride + ws1 * lws_stride + col];
-            if (nj.c2 >= d.T)
-                l += LSCp[(size_t)(nj.c2 - d.T) * 2 * lws_stride + ws2 * lws_stride + col];
-            lsc = l;
-            double* out = CLw + (size_t)(nj.node - d.T) * node_stride + wso * ws_stride + col;
+            lsc = l + lsc_f + lsc_o;
+            const int wso = nj.ws & 1;
+            double* out = CLp + (size_t)(nj.node - d.T) * node_stride + wso * ws_stride + col;
 #pragma unroll
-            for (int j = 0; j < kStates; ++j) out[j * j_stride] = y[j];
+            for (int j = 0; j < kStates; ++j) {
+                y[j] = acc[j];
+                out[j * j_stride] = acc[j];
+            }
             LSCp[(size_t)(nj.node - d.T) * 2 * lws_stride + wso * lws_stride + col] = lsc;
         }
+        prev = nj.node;
+        __syncwarp();
+    }
+    if (!ok) {
+        // Let any copy still in flight land before the CTA's shared memory is released.
+        if (lane == 0) {
+            mbar_wait_bounded(&bars[r][0], phase & 1);
+            mbar_wait_bounded(&bars[r][1], (phase >> 1) & 1);
+        }
+        bad = 1;
     }
     // Root reduction for this tile.
     if (cnt == 0 && valid) {
-        const double* x = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride + col;
+        const double* xp = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride + col;
 #pragma unroll
-        for (int j = 0; j < kStates; ++j) y[j] = x[j * j_stride];
+        for (int j = 0; j < kStates; ++j) y[j] = xp[j * j_stride];
         lsc = LSCp[(size_t)(h->root - d.T) * 2 * lws_stride + h->root_ws * lws_stride + col];
     }
     const double* rec =
@@ -198,39 +351,38 @@ __global__ void __launch_bounds__(kTileSites * R, (R <= 4 ? 2 : 1)) prune_kernel
         double s = 0.0;
 #pragma unroll
         for (int i = 0; i < kStates; ++i) s = fma(pi[i], y[i], s);
-        red[r][sl] = log(s) + lsc;
+        red[r][lane] = log(s) + lsc;
     }
     __syncthreads();
-    double v = 0.0;
-    if (r == 0 && valid) {
-        double mx = red[0][sl];
+    if (r == 0) {
+        double v = 0.0;
+        if (valid) {
+            double mx = red[0][lane];
 #pragma unroll
-        for (int rr = 1; rr < R; ++rr) mx = fmax(mx, red[rr][sl]);
-        double lse = mx;
-        if (mx > -INFINITY) {
-            double se = 0.0;
+            for (int rr = 1; rr < R; ++rr) mx = fmax(mx, red[rr][lane]);
+            double lse = mx;
+            if (mx > -INFINITY) {
+                double se = 0.0;
 #pragma unroll
-            for (int rr = 0; rr < R; ++rr) se += exp(red[rr][sl] - mx);
-            lse = mx + log(se);
+                for (int rr = 0; rr < R; ++rr) se += exp(red[rr][lane] - mx);
+                lse = mx + log(se);
+            }
+            // +I mixing, Particle.cpp:667-670, evaluated in log space.
+            const double pinv = h->pinv;
+            if (pinv > 0.0 && a.isinv[site] != 0) {
+                const double la = log1p(-pinv) + lse;
+                const double lb = log(pinv * pi[a.invchar[site]]);
+                const double m2 = fmax(la, lb);
+                v = m2 + log(exp(la - m2) + exp(lb - m2));
+            } else {
+                v = lse + log1p(-pinv);
+            }
+            if (bad) v = NAN;
+            a.site_lnl[(size_t)p * d.S + site] = v;
         }
-        // +I mixing, Particle.cpp:667-670, evaluated in log space.
-        const double pinv = h->pinv;
-        if (pinv > 0.0 && a.isinv[site] != 0) {
-            const double la = log1p(-pinv) + lse;
-            const double lb = log(pinv * pi[a.invchar[site]]);
-            const double m2 = fmax(la, lb);
-            v = m2 + log(exp(la - m2) + exp(lb - m2));
-        } else {
-            v = lse + log1p(-pinv);
-        }
-        a.site_lnl[(size_t)p * d.S + site] = v;
-    }
-    if (tid < kTileSites) {
         v = warp_sum(v);
-        if ((tid & 31) == 0) wsum[tid >> 5] = v;
+        if (lane == 0) a.partial[tile_id] = v;
     }
-    __syncthreads();
-    if (tid == 0) a.partial[tile_id] = wsum[0] + wsum[1];
 }
 
 __global__ void reduce_kernel(const int32_t* __restrict__ tile_off, const double* __restrict__ partial,
@@ -250,8 +402,8 @@ __global__ void accept_kernel(double* __restrict__ lnl, double* __restrict__ lnl
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const int p = first + i;
-    if (mask[i]) lnl_old[p] = lnl[p];
-    else lnl[p] = lnl_old[p];
+    if (mask[i] == 1) lnl_old[p] = lnl[p];
+    else if (mask[i] == 0) lnl[p] = lnl_old[p];
 }
 
 // ---------------------------------------------------------------------------
@@ -268,25 +420,38 @@ cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_prune(const PruneArgs& a, int ntiles, cudaStream_t st) {
+namespace {
+
+template <int R, int MINB>
+cudaError_t launch_prune_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
+    const size_t smem = sizeof(double) * 4 * (size_t)kPBlock * R;
+    cudaError_t e = cudaFuncSetAttribute(prune_kernel<R, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    prune_kernel<R, MINB><<<ntiles, 32 * R, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int prune_variants(int R) { return R == 4 ? 3 : 1; }
+
+cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
     if (ntiles <= 0) return cudaSuccess;
-    const size_t smem = sizeof(double) * 2 * a.d.R * kPBlock;
     switch (a.d.R) {
-#define SMCCAT_PRUNE_CASE(RR)                                                              \
-        case RR: {                                                                         \
-            cudaError_t e = cudaFuncSetAttribute(prune_kernel<RR>,                         \
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                                 (int)smem);                               \
-            if (e != cudaSuccess) return e;                                                \
-            prune_kernel<RR><<<ntiles, kTileSites * RR, smem, st>>>(a);                    \
-            break;                                                                         \
-        }
-        SMCCAT_PRUNE_CASE(1) SMCCAT_PRUNE_CASE(2) SMCCAT_PRUNE_CASE(3) SMCCAT_PRUNE_CASE(4)
-        SMCCAT_PRUNE_CASE(5) SMCCAT_PRUNE_CASE(6) SMCCAT_PRUNE_CASE(7) SMCCAT_PRUNE_CASE(8)
-#undef SMCCAT_PRUNE_CASE
+        case 1: return launch_prune_t<1, 4>(a, ntiles, st);
+        case 2: return launch_prune_t<2, 4>(a, ntiles, st);
+        case 3: return launch_prune_t<3, 4>(a, ntiles, st);
+        case 4:
+            if (variant == 1) return launch_prune_t<4, 3>(a, ntiles, st);
+            if (variant == 2) return launch_prune_t<4, 2>(a, ntiles, st);
+            return launch_prune_t<4, 4>(a, ntiles, st);
+        case 5: return launch_prune_t<5, 2>(a, ntiles, st);
+        case 6: return launch_prune_t<6, 2>(a, ntiles, st);
+        case 7: return launch_prune_t<7, 2>(a, ntiles, st);
+        case 8: return launch_prune_t<8, 2>(a, ntiles, st);
         default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 cudaError_t launch_reduce(const int32_t* tile_off, const double* partial, const PartHdr* hdr, int first,

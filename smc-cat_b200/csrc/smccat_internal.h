@@ -8,10 +8,11 @@
 //                                       reads 256 contiguous bytes per state
 //   LSC     [P][T-1][2][R][Spad]        cumulative log scale of each node's
 //                                       subtree (own scaler + children's)
-//   Pm      [P][Kmax][N][2][R][21][20]  transposed transition matrices: row j
-//                                       holds column j of P, row 20 holds the
-//                                       row sums (P applied to an all-ones
-//                                       tip vector for gap / X / ?)
+//   Pm      [P][Kmax][N][2][R][20][22]  transition matrices, row-major with a
+//                                       row stride of 22: column 20 holds the
+//                                       row sums (P applied to the all-ones
+//                                       tip vector of gap / X / ?), column 21
+//                                       is padding so rows are 16-byte aligned
 //   spec    [P][Kmax][2][SPEC_STRIDE]   eigenvalues, left/right factors, pi
 // Every workspace index (CL, P, spectral) is chosen by the host mirror and
 // shipped in the per-refresh plan, so accept/reject never touches the device.
@@ -27,10 +28,10 @@ void set_last_error(const std::string& msg);
 
 constexpr int kStates = 20;
 constexpr int kBase = 190;
-constexpr int kPRows = 21;                      // 20 columns of P + row sums
-constexpr int kPBlock = kPRows * kStates;       // 420 doubles per (node, rate)
+constexpr int kPCols = 22;                      // P row: 20 entries, row sum, pad
+constexpr int kPBlock = kStates * kPCols;       // 440 doubles per (node, rate)
 constexpr int kMaxRates = 8;
-constexpr int kTileSites = 64;                  // sites per pruning CTA
+constexpr int kTileSites = 32;                  // sites per pruning tile (one warp per rate)
 constexpr int kSpecStride = 20 + 400 + 400 + 20 + 8;  // lam, L, Rm, pi, pad
 
 // Offsets inside one spectral record.

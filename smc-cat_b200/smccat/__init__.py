@@ -92,6 +92,7 @@ def lib():
         "smccat_sync": ([vp], ctypes.c_int),
         "smccat_get_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
         "smccat_set_profiling": ([vp, _i32], ctypes.c_int),
+        "smccat_autotune": ([vp, _i32, _ip, _dp], ctypes.c_int),
         "smccat_get_profile": ([vp, ctypes.POINTER(Profile)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -272,6 +273,13 @@ class Engine:
         v = ctypes.c_void_p()
         _check(lib().smccat_get_stream(self._h, ctypes.byref(v)))
         return v.value or 0
+
+    def autotune(self, reps: int = 3) -> dict:
+        """Pick the fastest pruning-kernel variant on the loaded particles."""
+        v = ctypes.c_int32(0)
+        ms = np.full(8, np.nan)
+        _check(lib().smccat_autotune(self._h, int(reps), ctypes.byref(v), ms.ctypes.data_as(_dp)))
+        return {"variant": int(v.value), "ms": [float(x) for x in ms if not np.isnan(x)]}
 
     def set_profiling(self, enable: bool):
         _check(lib().smccat_set_profiling(self._h, 1 if enable else 0))

@@ -236,6 +236,21 @@ def test_two_refreshes_before_reject_restore_committed_state():
     eng.close()
 
 
+def test_autotune_keeps_likelihoods():
+    cfg = SMALL[1]
+    eng, codes, st = make_engine(cfg, 3, 41)
+    before = eng.lnl().copy()
+    res = eng.autotune(reps=1)
+    assert 0 <= res["variant"] < max(1, len(res["ms"]))
+    np.testing.assert_array_equal(eng.lnl(), before)
+    # edits and reject after the tuner's refreshes still restore the committed state
+    eng.set_branch_lengths(1, [0], [st["branch"][1, 0] * 2])
+    eng.refresh()
+    eng.accept(np.array([1, 0, 1], np.uint8))
+    np.testing.assert_array_equal(eng.lnl(), before)
+    eng.close()
+
+
 def test_protocol_errors():
     cfg = SMALL[0]
     eng, codes, st = make_engine(cfg, 2, 5)
