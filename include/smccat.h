@@ -203,6 +203,88 @@ int smccat_accept(smccat_ctx* ctx, int32_t first, int32_t count, const uint8_t* 
 /* Synchronise the context's stream. */
 int smccat_sync(smccat_ctx* ctx);
 
+/* ---- rejuvenation (MCMC) and the SMC weight step ------------------------ */
+
+/* Proposal tunables shared by the particles of a context: the public members
+ * of class Particle (Particle.hpp:87-94) and the DPP concentration
+ * (Particle.hpp:106). Defaults: 0.01, 1.0, 1.0, 1.0, 0.25, 0.25, 100.0, 0.01. */
+typedef struct smccat_tuning {
+    double adaptive_nni_epsilon;   /* aNNIEpsilon                          */
+    double shape_delta;            /* shapeDelta                           */
+    double scale_delta;            /* scaleDelta (one branch)              */
+    double subtree_scale_delta;    /* subtreeScaleDelta                    */
+    double stationary_delta;       /* stationaryDelta (logit shift sd)     */
+    double rate_matrix_delta;      /* rateMatrixDelta (single-entry move)  */
+    double invar_alpha;            /* invarAlpha (beta proposal concentration) */
+    double dpp_alpha;              /* dppAlpha                             */
+} smccat_tuning;
+
+int smccat_set_tuning(smccat_ctx* ctx, const smccat_tuning* t);
+int smccat_get_tuning(smccat_ctx* ctx, smccat_tuning* t);
+
+/* rateMatrixCholesky (Particle.hpp:93, set by main.cpp:267-289): lower
+ * triangular 190 x 190, row-major; default 0.5 I. */
+int smccat_set_rate_cholesky(smccat_ctx* ctx, const double* lower190x190);
+
+/* Split posterior probabilities for the adaptive NNI move
+ * (Tree::adaptiveNNIMove, Tree.cpp:673-766; computeSplitPosteriors,
+ * Miscellaneous.hpp:115-150). Split i is a taxon bit set in 2 words
+ * (bits[2i] holds taxa 0..63, bits[2i+1] taxa 64..127), canonicalised so that
+ * taxon 0 is set (Tree.cpp:511-516). Replaces the previous table. */
+int smccat_set_split_posteriors(smccat_ctx* ctx, int32_t n, const uint64_t* bits,
+                                const double* prob);
+
+/* Particle::lnPrior (Particle.cpp:484-517) of the current states. */
+int smccat_ln_prior(smccat_ctx* ctx, int32_t first, int32_t count, double* out);
+
+/* Move families of the reference's MCMC registry (main.cpp:55-106). */
+#define SMCCAT_FAMILY_TREE         0  /* treeMove: NNI / adaptive NNI / SPR / branch / subtree */
+#define SMCCAT_FAMILY_STATIONARY   1  /* stationaryMove                    */
+#define SMCCAT_FAMILY_SHAPE        2  /* shapeMove                         */
+#define SMCCAT_FAMILY_INVAR        3  /* invarMove                         */
+#define SMCCAT_FAMILY_RATE_MATRIX  4  /* rateMatrixMove                    */
+
+/* Move kinds, numbered like the reference's UpdateType (Particle.hpp:18-30). */
+#define SMCCAT_MOVE_ADAPTIVE_NNI        0
+#define SMCCAT_MOVE_NNI                 1
+#define SMCCAT_MOVE_SPR                 2
+#define SMCCAT_MOVE_BRANCH_LENGTH       3
+#define SMCCAT_MOVE_SCALE_SUBTREE       4
+#define SMCCAT_MOVE_INVAR               5
+#define SMCCAT_MOVE_RATE_SHAPE          6
+#define SMCCAT_MOVE_STATIONARY_SINGLE   7
+#define SMCCAT_MOVE_RATE_MATRIX_SINGLE  8
+#define SMCCAT_MOVE_RATE_MATRIX_FULL    9
+
+typedef struct smccat_move_stats {
+    uint64_t proposed[10];   /* per move kind (Particle::moveCount)         */
+    uint64_t accepted[10];   /* per move kind (Particle::acceptCount)       */
+    uint64_t lockstep_steps; /* batched refreshes issued                     */
+} smccat_move_stats;
+
+/* Apply one proposal of `family` to particle p (seeded), leaving it pending:
+ * the caller refreshes and accepts/rejects. Writes the move kind and the log
+ * Hastings ratio. The proposal half of one MH step of Mcmc::operator(). */
+int smccat_propose(smccat_ctx* ctx, int32_t p, int32_t family, uint64_t seed, int32_t* kind,
+                   double* hastings);
+
+/* Mcmc::operator()(particle, iterations, tempering) (Mcmc.cpp:25-73) for
+ * every particle of [first, first+count), all advancing in lockstep with one
+ * batched dirty refresh per MH step. Move weights and repeat counts follow the
+ * reference's registry (main.cpp:55-106): tree 3 x floor(T/4), stationary
+ * 1 x 2K, shape 1 x 2 (R > 1), invariant 1 x 2 (+I), rate matrix 1 x 5 (GTR).
+ * The particles must have no pending edits. */
+int smccat_rejuvenate(smccat_ctx* ctx, int32_t first, int32_t count, int32_t iterations,
+                      double temperature, uint64_t seed, smccat_move_stats* stats);
+
+/* computeNextStep (Miscellaneous.hpp:42-109) in FP64 on the device, on the
+ * current log-likelihoods of [first, first+count): bisects the temperature
+ * for `target_ess`, updates raw_weights in place and writes the normalised
+ * weights, the new temperature and the ESS. */
+int smccat_smc_step(smccat_ctx* ctx, int32_t first, int32_t count, double* raw_weights,
+                    double target_ess, double last_temp, double* cur_temp, double* ess,
+                    double* norm_weights);
+
 /* ---- measurement (no reference counterpart: the reference only has the
  * compile-time TIME_PROFILE wall-clock prints, Particle.cpp:533-631) ----- */
 

@@ -39,8 +39,6 @@ int fail(int code, const std::string& msg) {
 
 void smccat::set_last_error(const std::string& msg) { g_err = msg; }
 
-namespace {
-
 #define CK(call)                                                                      \
     do {                                                                              \
         cudaError_t e_ = (call);                                                      \
@@ -48,33 +46,8 @@ namespace {
             return fail(SMCCAT_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-struct Mirror {
-    std::vector<int32_t> parent;   // N
-    std::vector<double> branch;    // N
-    std::vector<int32_t> kids;     // 2N, -1 for tips
-    std::vector<int32_t> post;     // internal nodes, post-order (root last)
-    int root = -1;
-    std::vector<double> base;      // 190
-    int K = 0;
-    std::vector<double> logits;    // Kmax * 20
-    double pinv = 0.0, shape = 1.0;
-    double rates[kMaxRates] = {1, 1, 1, 1, 1, 1, 1, 1};
-    std::vector<uint8_t> clws, pws;  // N
-    std::vector<uint8_t> sws;        // Kmax
-};
+#include "engine_internal.h"
 
-struct Slot {
-    Mirror cur, old;
-    std::vector<int32_t> assign;
-    std::vector<uint8_t> dirty_cl, dirty_p, dirty_spec;
-    bool loaded = false;
-    bool full = false;          // next refresh rebuilds everything
-    bool commit_on_refresh = false;
-    bool pending = false;       // edits since the last commit
-    bool refreshed = false;     // refreshed since the last commit
-};
-
-}  // namespace
 
 struct smccat_ctx {
     smccat_config cfg{};
@@ -284,6 +257,7 @@ int smccat_lg_exchangeabilities(double* out190) {
 
 int smccat_destroy(smccat_ctx* c) {
     if (!c) return SMCCAT_OK;
+    mcmc_release(c);
     cudaSetDevice(c->cfg.device);
     if (c->st) cudaStreamSynchronize(c->st);
     void* dptrs[] = {c->d_codes, c->d_isinv, c->d_invchar, c->d_perm, c->d_tiles, c->d_tile_off,
@@ -515,6 +489,12 @@ int smccat_get_particles(smccat_ctx* c, int32_t first, int32_t count, int32_t* p
 }
 
 int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
+    return refresh_internal(c, first, count, mode, nullptr);
+}
+
+}  // extern "C"
+
+int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, const uint8_t* active) {
     int rc = check_range(c, first, count);
     if (rc) return rc;
     if (count == 0) return SMCCAT_OK;
@@ -522,6 +502,7 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
         return fail(SMCCAT_EINVAL, "unknown refresh mode");
     for (int i = 0; i < count; ++i)
         if (!c->slots[first + i].loaded) return fail(SMCCAT_ESTATE, "particle has no state loaded");
+    auto on = [&](int i) { return !active || active[i]; };
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaEventSynchronize(c->plan_done));  // previous plan copy has left the pinned buffer
     const Dims& d = c->d;
@@ -544,6 +525,7 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
     int nn = 0;
     for (int i = 0; i < count; ++i) {
         const Slot& s = c->slots[first + i];
+        if (!on(i)) continue;
         const bool full = (mode == SMCCAT_REFRESH_FULL) || s.full;
         if (full) nn += (int)s.cur.post.size();
         else for (int n : s.cur.post) nn += s.dirty_cl[n];
@@ -555,6 +537,7 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
     int np_ = 0;
     for (int i = 0; i < count; ++i) {
         const Slot& s = c->slots[first + i];
+        if (!on(i)) continue;
         const bool full = (mode == SMCCAT_REFRESH_FULL) || s.full;
         if (full) np_ += N - 1;
         else for (int n = 0; n < N; ++n) np_ += (s.dirty_p[n] && n != s.cur.root);
@@ -570,6 +553,12 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
         const int p = first + i;
         Slot& s = c->slots[p];
         Mirror& m = s.cur;
+        if (!on(i)) {
+            PartHdr& h = hdr[i];
+            std::memset(&h, 0, sizeof(h));
+            h.node_off = nn;
+            continue;
+        }
         const bool full = (mode == SMCCAT_REFRESH_FULL) || s.full;
         if (full) {
             std::fill(s.dirty_spec.begin(), s.dirty_spec.begin() + m.K, 1);
@@ -663,10 +652,11 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
 
     // Loaded particles commit their first refresh (copyFromSerialized does).
     bool any_commit = false;
-    for (int i = 0; i < count; ++i) any_commit |= c->slots[first + i].commit_on_refresh;
+    for (int i = 0; i < count; ++i) any_commit |= on(i) && c->slots[first + i].commit_on_refresh;
     if (any_commit) {
         uint8_t* mask = reinterpret_cast<uint8_t*>(c->h_plan + plan_bytes);
-        for (int i = 0; i < count; ++i) mask[i] = c->slots[first + i].commit_on_refresh ? 1 : 2;
+        for (int i = 0; i < count; ++i)
+            mask[i] = (on(i) && c->slots[first + i].commit_on_refresh) ? 1 : 2;
         // The mask shares the pinned plan buffer; its copy precedes plan_done.
         uint8_t* d_mask = reinterpret_cast<uint8_t*>(c->d_plan + plan_bytes);
         CK(h2d(c, d_mask, mask, count));
@@ -675,7 +665,7 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
                   [&] { return launch_accept(c->d_lnl, c->d_lnl_old, d_mask, first, count, c->st); }));
         for (int i = 0; i < count; ++i) {
             Slot& s = c->slots[first + i];
-            if (!s.commit_on_refresh) continue;
+            if (!on(i) || !s.commit_on_refresh) continue;
             s.old = s.cur;
             s.commit_on_refresh = false;
             s.pending = false;
@@ -693,6 +683,13 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
     }
     return SMCCAT_OK;
 }
+
+const Slot& smccat::slot_of(const smccat_ctx* c, int p) { return c->slots[p]; }
+const Dims& smccat::dims_of(const smccat_ctx* c) { return c->d; }
+int smccat::model_flags_of(const smccat_ctx* c) { return c->cfg.model_flags; }
+const double* smccat::lnl_device(const smccat_ctx* c) { return c->d_lnl; }
+
+extern "C" {
 
 int smccat_get_lnl(smccat_ctx* c, int32_t first, int32_t count, double* out) {
     int rc = check_range(c, first, count);

@@ -1,0 +1,56 @@
+// Internal state of the host engine, shared by the C-ABI implementation
+// (engine.cu) and the MCMC driver (mcmc.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "kernels.h"
+#include "smccat.h"
+
+namespace smccat {
+
+// Host mirror of one particle's state and of its device workspace indices.
+struct Mirror {
+    std::vector<int32_t> parent;   // N
+    std::vector<double> branch;    // N
+    std::vector<int32_t> kids;     // 2N, -1 for tips
+    std::vector<int32_t> post;     // internal nodes, post-order (root last)
+    int root = -1;
+    std::vector<double> base;      // 190
+    int K = 0;
+    std::vector<double> logits;    // Kmax * 20
+    double pinv = 0.0, shape = 1.0;
+    double rates[kMaxRates] = {1, 1, 1, 1, 1, 1, 1, 1};
+    std::vector<uint8_t> clws, pws;  // N
+    std::vector<uint8_t> sws;        // Kmax
+};
+
+struct Slot {
+    Mirror cur, old;
+    std::vector<int32_t> assign;
+    std::vector<uint8_t> dirty_cl, dirty_p, dirty_spec;
+    bool loaded = false;
+    bool full = false;          // next refresh rebuilds everything
+    bool commit_on_refresh = false;
+    bool pending = false;       // edits since the last commit
+    bool refreshed = false;     // refreshed since the last commit
+};
+
+// Refresh particles [first, first+count); `active` (count bytes, may be
+// null) excludes particles from the launch without touching their state.
+int refresh_internal(smccat_ctx* c, int first, int count, int mode, const uint8_t* active);
+
+// Host mirror of one slot (read-only view for the MCMC driver).
+const Slot& slot_of(const smccat_ctx* c, int p);
+const Dims& dims_of(const smccat_ctx* c);
+int model_flags_of(const smccat_ctx* c);
+const double* lnl_device(const smccat_ctx* c);  // [max_particles] current log-likelihoods
+
+// Drop the MCMC settings kept for a context (called by smccat_destroy).
+void mcmc_release(const smccat_ctx* c);
+
+}  // namespace smccat

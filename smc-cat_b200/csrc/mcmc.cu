@@ -1,0 +1,626 @@
+// Rejuvenation MCMC driver and SMC weight step of the B200 engine.
+//
+// The reference runs Mcmc::operator() (Mcmc.cpp:25-73) once per particle,
+// particles spread over OpenMP threads (main.cpp:295-312), and every MH step
+// calls refreshLikelihood() on that one particle. Here all particles of a
+// range advance in lockstep: at every step each unfinished particle makes its
+// next proposal on the host mirror (the reference's move rules, Tree.cpp and
+// Particle.cpp), one batched dirty refresh evaluates every proposal on the
+// device, and the MH test (tempered likelihood + lnPrior + Hastings) decides
+// per particle; accept/reject only flips workspace indices.
+//
+// computeNextStep (Miscellaneous.hpp:42-109) runs on the device in FP64 on
+// the log-likelihoods already resident there.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <random>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "engine_internal.h"
+#include "host_math.h"
+#include "smccat.h"
+
+namespace smccat {
+namespace {
+
+int mfail(int code, const std::string& msg) {
+    set_last_error(msg);
+    return code;
+}
+
+// Move kinds in the reference's UpdateType order (Particle.hpp:18-30).
+enum Kind {
+    ADAPTIVE_NNI = 0, NNI = 1, SPR = 2, BRANCH_LENGTH = 3, SCALE_SUBTREE = 4, INVAR = 5,
+    RATE_SHAPE = 6, STATIONARY_SINGLE = 7, RATE_MATRIX_SINGLE = 8, RATE_MATRIX_FULL = 9
+};
+
+// Registry entries of main.cpp:55-106.
+enum Family { FAM_TREE, FAM_STATIONARY, FAM_SHAPE, FAM_INVAR, FAM_RATE_MATRIX };
+
+struct Split {
+    uint64_t w[2];
+    bool operator==(const Split& o) const { return w[0] == o.w[0] && w[1] == o.w[1]; }
+};
+struct SplitHash {
+    size_t operator()(const Split& s) const { return std::hash<uint64_t>()(s.w[0] * 0x9E3779B97F4A7C15ull ^ s.w[1]); }
+};
+
+struct Tuning {
+    smccat_tuning t;
+    std::vector<double> chol;  // 190 x 190 lower triangular, row-major
+    std::unordered_map<Split, double, SplitHash> split_post;
+};
+
+std::unordered_map<const smccat_ctx*, Tuning>& tunings() {
+    static std::unordered_map<const smccat_ctx*, Tuning> m;
+    return m;
+}
+
+std::mutex& tunings_mu() {
+    static std::mutex mu;
+    return mu;
+}
+
+// Per-context MCMC settings (entries stay valid: unordered_map never moves
+// its nodes; a context's entry is erased by smccat_destroy).
+Tuning& tuning_of(const smccat_ctx* c) {
+    std::lock_guard<std::mutex> lk(tunings_mu());
+    auto& m = tunings();
+    auto it = m.find(c);
+    if (it != m.end()) return it->second;
+    Tuning tn;
+    tn.t = smccat_tuning{0.01, 1.0, 1.0, 1.0, 0.25, 0.25, 100.0, 0.01};  // Particle.hpp:87-94, 106
+    tn.chol.assign(190 * 190, 0.0);
+    for (int i = 0; i < 190; ++i) tn.chol[i * 190 + i] = 0.5;         // Particle.hpp:93
+    return m.emplace(c, std::move(tn)).first->second;
+}
+
+using Rng = std::mt19937_64;
+
+double unif(Rng& g) { return std::generate_canonical<double, 53>(g); }
+
+double normal(Rng& g, double sd) { return std::normal_distribution<double>(0.0, sd)(g); }
+
+double beta_draw(Rng& g, double a, double b) {
+    const double x = std::gamma_distribution<double>(a, 1.0)(g);
+    const double y = std::gamma_distribution<double>(b, 1.0)(g);
+    return x / (x + y);
+}
+
+double beta_lpdf(double x, double a, double b) {
+    return std::lgamma(a + b) - std::lgamma(a) - std::lgamma(b) + (a - 1.0) * std::log(x) +
+           (b - 1.0) * std::log1p(-x);
+}
+
+double gamma_lpdf(double x, double shape, double scale) {
+    return (shape - 1.0) * std::log(x) - x / scale - std::lgamma(shape) - shape * std::log(scale);
+}
+
+double normal_lpdf(double z) { return -0.5 * z * z - 0.91893853320467274178; }
+
+// Working copy of one particle's tree with child lists in id order.
+struct WTree {
+    int T, N, root;
+    std::vector<int32_t> parent;
+    std::vector<double> branch;
+    std::vector<int32_t> kids;  // 2 per node
+    void load(const Mirror& m, int T_) {
+        T = T_;
+        N = 2 * T - 1;
+        root = m.root;
+        parent = m.parent;
+        branch = m.branch;
+        kids = m.kids;
+    }
+    void rebuild_kids() {
+        std::vector<int> nk(N, 0);
+        std::fill(kids.begin(), kids.end(), -1);
+        for (int n = 0; n < N; ++n)
+            if (parent[n] >= 0) kids[2 * parent[n] + nk[parent[n]]++] = n;
+        for (int n = T; n < N; ++n)
+            if (kids[2 * n] > kids[2 * n + 1]) std::swap(kids[2 * n], kids[2 * n + 1]);
+    }
+    bool in_subtree(int x, int r) const {  // Tree.hpp:29-34
+        for (; x >= 0; x = parent[x])
+            if (x == r) return true;
+        return false;
+    }
+    int uniform_node(Rng& g) const { return std::min(N - 1, (int)(unif(g) * N)); }
+    // chooseNodeFromSet (Tree.cpp:614-623) over the (ordered) children of n.
+    int choose_child(Rng& g, int n) const { return kids[2 * n + std::min(1, (int)(unif(g) * 2))]; }
+    // Clade bit sets of every node, canonicalised so that taxon 0 is set
+    // (Tree.cpp:485-519).
+    std::vector<Split> splits() const {
+        std::vector<Split> s(N, Split{{0, 0}});
+        std::vector<int> order;
+        order.reserve(N);
+        std::vector<int> st{root};
+        while (!st.empty()) {
+            const int n = st.back();
+            st.pop_back();
+            order.push_back(n);
+            if (n >= T) { st.push_back(kids[2 * n]); st.push_back(kids[2 * n + 1]); }
+        }
+        for (int i = N - 1; i >= 0; --i) {
+            const int n = order[i];
+            if (n < T) s[n].w[n >> 6] |= 1ull << (n & 63);
+            else for (int c = 0; c < 2; ++c) {
+                s[n].w[0] |= s[kids[2 * n + c]].w[0];
+                s[n].w[1] |= s[kids[2 * n + c]].w[1];
+            }
+        }
+        Split full{{0, 0}};
+        for (int t = 0; t < T; ++t) full.w[t >> 6] |= 1ull << (t & 63);
+        for (auto& x : s)
+            if (!(x.w[0] & 1ull)) { x.w[0] = ~x.w[0] & full.w[0]; x.w[1] = ~x.w[1] & full.w[1]; }
+        return s;
+    }
+};
+
+int popcount2(const Split& s) { return __builtin_popcountll(s.w[0]) + __builtin_popcountll(s.w[1]); }
+
+// Adaptive-NNI node weights (Tree.cpp:676-694): epsilon + (1 - posterior of
+// the node's split), or epsilon + 1 when the split is absent or trivial.
+std::vector<double> annI_weights(const WTree& t, const Tuning& tn, double* total) {
+    std::vector<double> w(t.N, 0.0);
+    const auto sp = t.splits();
+    *total = 0.0;
+    for (int n = t.T; n < t.N; ++n) {
+        if (n == t.root) continue;
+        double v = tn.t.adaptive_nni_epsilon;
+        const int cnt = popcount2(sp[n]);
+        auto it = (cnt == 1 || cnt == t.T - 1) ? tn.split_post.end() : tn.split_post.find(sp[n]);
+        v += (it != tn.split_post.end()) ? 1.0 - it->second : 1.0;
+        w[n] = v;
+        *total += v;
+    }
+    return w;
+}
+
+struct Proposal {
+    int kind = -1;
+    double hastings = 0.0;
+};
+
+// One proposal on particle p (Particle::treeMove etc.), applied through the
+// engine's edit calls so the dirty sets follow.
+int propose(smccat_ctx* c, int p, int family, Rng& g, const Tuning& tn, Proposal* out) {
+    const Slot& s = slot_of(c, p);
+    const Mirror& m = s.cur;
+    const Dims& d = dims_of(c);
+    out->hastings = 0.0;
+    if (family == FAM_TREE) {
+        WTree t;
+        t.load(m, d.T);
+        const double u = unif(g);  // Particle.cpp:680-701
+        if (u < 0.5 && u >= 0.4) {  // SPR, Tree.cpp:768-812
+            int x;
+            do { x = t.uniform_node(g); } while (x == t.root || x < t.T);
+            const int sch = t.choose_child(g, x);
+            const int sib = (t.kids[2 * x] == sch) ? t.kids[2 * x + 1] : t.kids[2 * x];
+            int a;
+            do { a = t.uniform_node(g); } while (t.in_subtree(a, x) || a == t.root);
+            const int a_par = t.parent[a];
+            const int gpar = t.parent[x];
+            t.parent[sib] = gpar;
+            t.parent[x] = (a_par == x) ? gpar : a_par;
+            t.parent[a] = x;
+            out->kind = SPR;
+            return smccat_set_topology(c, p, t.parent.data(), t.branch.data());
+        }
+        if (u < 0.4) {  // NNI (u < 0.1) or adaptive NNI, Tree.cpp:625-766
+            int x;
+            double sel = 0.0, tot = 0.0;
+            std::vector<double> w;
+            if (u < 0.1) {
+                do { x = t.uniform_node(g); } while (x == t.root || x < t.T);
+                out->kind = NNI;
+            } else {
+                w = annI_weights(t, tn, &tot);
+                const double r = unif(g);
+                double cum = 0.0;
+                x = -1;
+                for (int n = t.T; n < t.N; ++n) {
+                    if (n == t.root) continue;
+                    cum += w[n] / tot;
+                    x = n;
+                    if (r <= cum) break;
+                }
+                sel = w[x] / tot;
+                out->kind = ADAPTIVE_NNI;
+            }
+            const int a = t.parent[x];
+            const int n1 = t.choose_child(g, x);
+            (void)unif(g);  // the reference draws from the one-element sibling set too
+            const int n2 = (t.kids[2 * a] == x) ? t.kids[2 * a + 1] : t.kids[2 * a];
+            t.parent[n1] = a;
+            t.parent[n2] = x;
+            if (out->kind == ADAPTIVE_NNI) {
+                t.rebuild_kids();
+                double tot2 = 0.0;
+                const auto w2 = annI_weights(t, tn, &tot2);
+                out->hastings = std::log(w2[x] / tot2) - std::log(sel);
+            }
+            return smccat_set_topology(c, p, t.parent.data(), t.branch.data());
+        }
+        int x;
+        do { x = t.uniform_node(g); } while (x == t.root);
+        if (u < 0.9) {  // scaleBranchMove, Tree.cpp:553-578
+            const double sc = std::exp(tn.t.scale_delta * (unif(g) - 0.5));
+            const double nb = t.branch[x] * sc;
+            out->kind = BRANCH_LENGTH;
+            out->hastings = std::log(sc);
+            return smccat_set_branch_lengths(c, p, 1, &x, &nb);
+        }
+        // scaleSubtreeMove, Tree.cpp:580-612
+        const double sc = std::exp(tn.t.subtree_scale_delta * (unif(g) - 0.5));
+        std::vector<int32_t> nodes;
+        std::vector<double> lens;
+        std::vector<int> st{x};
+        while (!st.empty()) {
+            const int n = st.back();
+            st.pop_back();
+            nodes.push_back(n);
+            lens.push_back(t.branch[n] * sc);
+            if (n >= t.T) { st.push_back(t.kids[2 * n]); st.push_back(t.kids[2 * n + 1]); }
+        }
+        out->kind = SCALE_SUBTREE;
+        out->hastings = nodes.size() * std::log(sc);
+        return smccat_set_branch_lengths(c, p, (int)nodes.size(), nodes.data(), lens.data());
+    }
+    if (family == FAM_STATIONARY) {
+        // Particle::stationaryMove (Particle.cpp:734-742) with the shift applied
+        // to the class's logit: the reference shifts pi and then recomputes pi
+        // from the unchanged logits, which makes its move a no-op.
+        const int k = std::min(m.K - 1, (int)(unif(g) * m.K));
+        const int i = std::min(19, (int)(unif(g) * 20));
+        double lg[kStates];
+        std::memcpy(lg, &m.logits[(size_t)k * kStates], sizeof(lg));
+        lg[i] += normal(g, tn.t.stationary_delta);
+        out->kind = STATIONARY_SINGLE;
+        return smccat_set_class_logits(c, p, k, lg);
+    }
+    if (family == FAM_SHAPE) {  // Particle::shapeMove, Particle.cpp:768-783
+        const double sc = std::exp(tn.t.shape_delta * (unif(g) - 0.5));
+        out->kind = RATE_SHAPE;
+        out->hastings = std::log(sc);
+        return smccat_set_shape(c, p, m.shape * sc);
+    }
+    if (family == FAM_INVAR) {  // Particle::invarMove, Particle.cpp:744-766
+        const double al = tn.t.invar_alpha;
+        const double cur = m.pinv;
+        const double a = al + 1.0, b = al / cur - a + 2.0;
+        double nv = beta_draw(g, a, b);
+        nv = std::min(std::max(nv, 1e-300), 1.0 - 1e-16);
+        const double b2 = al / nv - a + 2.0;
+        out->kind = INVAR;
+        out->hastings = beta_lpdf(cur, a, b2) - beta_lpdf(nv, a, b);
+        return smccat_set_pinv(c, p, nv);
+    }
+    // Particle::rateMatrixMove (Particle.cpp:706-732); the new exchangeabilities
+    // take effect at once (the reference only updates its eigensystems later).
+    std::vector<double> base = m.base;
+    if (unif(g) < 0.25) {
+        double z[kBase];
+        for (int i = 0; i < kBase; ++i) z[i] = normal(g, 1.0);
+        for (int i = 0; i < kBase; ++i) {
+            double sacc = 0.0;
+            for (int j = 0; j <= i; ++j) sacc += tn.chol[i * kBase + j] * z[j];
+            base[i] += sacc;
+        }
+        out->kind = RATE_MATRIX_FULL;
+    } else {
+        const int i = std::min(kBase - 1, (int)(kBase * unif(g)));
+        base[i] += normal(g, 1.0) * tn.t.rate_matrix_delta;
+        out->kind = RATE_MATRIX_SINGLE;
+    }
+    return smccat_set_base(c, p, base.data());
+}
+
+// Particle::lnPrior (Particle.cpp:484-517) of the current mirror state.
+double ln_prior(const smccat_ctx* c, int p, const Tuning& tn) {
+    const Slot& s = slot_of(c, p);
+    const Mirror& m = s.cur;
+    const Dims& d = dims_of(c);
+    double len = 0.0;
+    for (int n = 0; n < d.N; ++n) len += m.branch[n];
+    double lnp = gamma_lpdf(len, (double)(d.N - 1), 0.1);
+    if (d.R > 1) lnp += gamma_lpdf(m.shape, 3.0, 2.0);
+    if (!(model_flags_of(c) & SMCCAT_MODEL_LG))
+        for (int i = 0; i < kBase; ++i) lnp += normal_lpdf(m.base[i]);
+    std::vector<int> cnt(m.K, 0);
+    for (int v : s.assign) cnt[v]++;
+    const double alpha = tn.t.dpp_alpha;
+    int kk = 0;
+    for (int k = 0; k < m.K; ++k) {
+        if (cnt[k] == 0) continue;  // an empty class carries no prior mass
+        ++kk;
+        for (int i = 0; i < kStates; ++i) lnp += normal_lpdf(m.logits[(size_t)k * kStates + i]);
+        lnp += std::lgamma((double)cnt[k]);
+    }
+    lnp += std::log(alpha) * kk;
+    lnp += std::lgamma(alpha) - std::lgamma(alpha + d.S);
+    return lnp;
+}
+
+// ---------------------------------------------------------------------------
+// computeNextStep on the device: one CTA, fixed-order FP64 reductions.
+constexpr int kStepThreads = 1024;
+
+__device__ double block_reduce(double v, double* sh, bool is_max) {
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int o = kStepThreads / 2; o > 0; o >>= 1) {
+        if (t < o) sh[t] = is_max ? fmax(sh[t], sh[t + o]) : sh[t] + sh[t + o];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ double ess_at(const double* w, const double* lnl, int n, double temp, double last,
+                         double* sh) {
+    double mx = -INFINITY;
+    for (int i = threadIdx.x; i < n; i += kStepThreads) mx = fmax(mx, w[i] + (temp - last) * lnl[i]);
+    mx = block_reduce(mx, sh, true);
+    double tot = 0.0;
+    for (int i = threadIdx.x; i < n; i += kStepThreads) tot += exp(w[i] + (temp - last) * lnl[i] - mx);
+    tot = block_reduce(tot, sh, false);
+    double sq = 0.0;
+    for (int i = threadIdx.x; i < n; i += kStepThreads) {
+        const double e = exp(w[i] + (temp - last) * lnl[i] - mx) / tot;
+        sq += e * e;
+    }
+    sq = block_reduce(sq, sh, false);
+    return 1.0 / sq;
+}
+
+__global__ void __launch_bounds__(kStepThreads) smc_step_kernel(double* w, const double* lnl, int n,
+                                                                double target, double last,
+                                                                double* normw, double* out) {
+    __shared__ double sh[kStepThreads];
+    double low = last, high = 1.0;
+    for (int it = 0; it < 200 && high - low > 1e-5; ++it) {
+        const double mid = 0.5 * (low + high);
+        if (ess_at(w, lnl, n, mid, last, sh) > target) low = mid;
+        else high = mid;
+    }
+    const double temp = high;
+    for (int i = threadIdx.x; i < n; i += kStepThreads) w[i] = w[i] + (temp - last) * lnl[i];
+    __syncthreads();
+    double mx = -INFINITY;
+    for (int i = threadIdx.x; i < n; i += kStepThreads) mx = fmax(mx, w[i]);
+    mx = block_reduce(mx, sh, true);
+    double tot = 0.0;
+    for (int i = threadIdx.x; i < n; i += kStepThreads) tot += exp(w[i] - mx);
+    tot = block_reduce(tot, sh, false);
+    double sq = 0.0;
+    for (int i = threadIdx.x; i < n; i += kStepThreads) {
+        const double e = exp(w[i] - mx) / tot;
+        normw[i] = e;
+        sq += e * e;
+    }
+    sq = block_reduce(sq, sh, false);
+    if (threadIdx.x == 0) { out[0] = temp; out[1] = 1.0 / sq; }
+}
+
+}  // namespace
+
+void mcmc_release(const smccat_ctx* c) {
+    std::lock_guard<std::mutex> lk(tunings_mu());
+    tunings().erase(c);
+}
+
+}  // namespace smccat
+
+using namespace smccat;
+
+extern "C" {
+
+int smccat_set_tuning(smccat_ctx* c, const smccat_tuning* t) {
+    if (!c || !t) return mfail(SMCCAT_EINVAL, "null argument");
+    if (!(t->invar_alpha > 0.0) || !(t->dpp_alpha > 0.0)) return mfail(SMCCAT_EINVAL, "bad tuning");
+    tuning_of(c).t = *t;
+    return SMCCAT_OK;
+}
+
+int smccat_get_tuning(smccat_ctx* c, smccat_tuning* t) {
+    if (!c || !t) return mfail(SMCCAT_EINVAL, "null argument");
+    *t = tuning_of(c).t;
+    return SMCCAT_OK;
+}
+
+int smccat_set_rate_cholesky(smccat_ctx* c, const double* lower190) {
+    if (!c || !lower190) return mfail(SMCCAT_EINVAL, "null argument");
+    auto& ch = tuning_of(c).chol;
+    for (int i = 0; i < 190; ++i)
+        for (int j = 0; j < 190; ++j) ch[i * 190 + j] = (j <= i) ? lower190[i * 190 + j] : 0.0;
+    return SMCCAT_OK;
+}
+
+int smccat_set_split_posteriors(smccat_ctx* c, int32_t n, const uint64_t* bits, const double* prob) {
+    if (!c || n < 0 || (n > 0 && (!bits || !prob))) return mfail(SMCCAT_EINVAL, "null argument");
+    auto& mp = tuning_of(c).split_post;
+    mp.clear();
+    for (int i = 0; i < n; ++i) mp[Split{{bits[2 * i], bits[2 * i + 1]}}] = prob[i];
+    return SMCCAT_OK;
+}
+
+int smccat_ln_prior(smccat_ctx* c, int32_t first, int32_t count, double* out) {
+    if (!c || !out) return mfail(SMCCAT_EINVAL, "null argument");
+    const Tuning& tn = tuning_of(c);
+    for (int i = 0; i < count; ++i) {
+        const Slot& s = slot_of(c, first + i);
+        if (!s.loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
+        out[i] = ln_prior(c, first + i, tn);
+    }
+    return SMCCAT_OK;
+}
+
+int smccat_propose(smccat_ctx* c, int32_t p, int32_t family, uint64_t seed, int32_t* kind,
+                   double* hastings) {
+    if (!c) return mfail(SMCCAT_EINVAL, "null context");
+    if (p < 0 || !slot_of(c, p).loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
+    if (family < SMCCAT_FAMILY_TREE || family > SMCCAT_FAMILY_RATE_MATRIX)
+        return mfail(SMCCAT_EINVAL, "unknown move family");
+    if (family == SMCCAT_FAMILY_INVAR && !(slot_of(c, p).cur.pinv > 0.0))
+        return mfail(SMCCAT_EINVAL, "invariant-site move needs pinv > 0");
+    Rng g(seed);
+    Proposal pr;
+    const int rc = propose(c, p, family, g, tuning_of(c), &pr);
+    if (rc) return rc;
+    if (kind) *kind = pr.kind;
+    if (hastings) *hastings = pr.hastings;
+    return SMCCAT_OK;
+}
+
+int smccat_rejuvenate(smccat_ctx* c, int32_t first, int32_t count, int32_t iterations,
+                      double temperature, uint64_t seed, smccat_move_stats* stats) {
+    if (!c) return mfail(SMCCAT_EINVAL, "null context");
+    if (iterations < 0 || count < 0 || first < 0) return mfail(SMCCAT_EINVAL, "bad range");
+    const Dims& d = dims_of(c);
+    const int flags = model_flags_of(c);
+    const Tuning& tn = tuning_of(c);
+    for (int i = 0; i < count; ++i) {
+        const Slot& s = slot_of(c, first + i);
+        if (!s.loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
+        if (s.pending) return mfail(SMCCAT_ESTATE, "particle has uncommitted edits");
+    }
+    // The move registry of main.cpp:55-106: (weight, repeat count, family).
+    struct Entry { double w; int family; };
+    std::vector<Entry> reg{{3.0, FAM_TREE}, {1.0, FAM_STATIONARY}};
+    if (d.R > 1) reg.push_back({1.0, FAM_SHAPE});
+    if (flags & SMCCAT_MODEL_INVAR) reg.push_back({1.0, FAM_INVAR});
+    if (!(flags & SMCCAT_MODEL_LG)) reg.push_back({1.0, FAM_RATE_MATRIX});
+    double wt = 0.0;
+    for (auto& e : reg) wt += e.w;
+    std::vector<double> cum;  // Mcmc::initMoveProbs, Mcmc.cpp:15-23
+    double acc = 0.0;
+    for (auto& e : reg) { acc += e.w; cum.push_back(acc / wt); }
+    auto repeats = [&](int family, int p) -> int {
+        switch (family) {
+            case FAM_TREE: return (int)(d.T * 0.25);
+            case FAM_STATIONARY: return slot_of(c, p).cur.K * 2;
+            case FAM_SHAPE: return 2;
+            case FAM_INVAR: return 2;
+            default: return 5;
+        }
+    };
+    struct PS {
+        Rng g;
+        int iter = 0, family = 0, left = 0;
+        bool done = false;
+        double lik = 0.0, prior = 0.0;
+        Proposal pr;
+    };
+    std::vector<PS> ps(count);
+    for (int i = 0; i < count; ++i) ps[i].g.seed(seed * 0x9E3779B97F4A7C15ull + (uint64_t)(first + i) + 1);
+    smccat_move_stats st{};
+    // Mcmc.cpp:34-37: current likelihood (root reduction) and prior.
+    int rc = refresh_internal(c, first, count, SMCCAT_REFRESH_DIRTY, nullptr);
+    if (rc) return rc;
+    std::vector<double> lnl(count);
+    rc = smccat_get_lnl(c, first, count, lnl.data());
+    if (rc) return rc;
+    for (int i = 0; i < count; ++i) {
+        ps[i].lik = lnl[i] * temperature;
+        ps[i].prior = ln_prior(c, first + i, tn);
+    }
+    std::vector<uint8_t> active(count), mask(count);
+    for (;;) {
+        int n_active = 0;
+        for (int i = 0; i < count; ++i) {
+            PS& q = ps[i];
+            active[i] = 0;
+            while (!q.done && q.left == 0) {
+                if (q.iter == iterations) { q.done = true; break; }
+                const double u = unif(q.g);  // Mcmc.cpp:40-50
+                int j = 0;
+                while (j + 1 < (int)cum.size() && !(u < cum[j])) ++j;
+                q.family = reg[j].family;
+                q.left = repeats(q.family, first + i);
+                q.iter++;
+            }
+            if (q.done) continue;
+            rc = propose(c, first + i, q.family, q.g, tn, &q.pr);
+            if (rc) return rc;
+            q.left--;
+            active[i] = 1;
+            ++n_active;
+        }
+        if (n_active == 0) break;
+        rc = refresh_internal(c, first, count, SMCCAT_REFRESH_DIRTY, active.data());
+        if (rc) return rc;
+        rc = smccat_get_lnl(c, first, count, lnl.data());
+        if (rc) return rc;
+        st.lockstep_steps++;
+        for (int i = 0; i < count; ++i) {
+            mask[i] = 1;
+            if (!active[i]) continue;
+            PS& q = ps[i];
+            const double nprior = ln_prior(c, first + i, tn);
+            const double nlik = lnl[i] * temperature;
+            const double ratio = (nprior + nlik) - (q.prior + q.lik) + q.pr.hastings;  // Mcmc.cpp:57-60
+            const bool ok = std::log(unif(q.g)) <= ratio;
+            mask[i] = ok ? 1 : 0;
+            st.proposed[q.pr.kind]++;
+            if (ok) {
+                st.accepted[q.pr.kind]++;
+                q.prior = nprior;
+                q.lik = nlik;
+            }
+        }
+        rc = smccat_accept(c, first, count, mask.data());
+        if (rc) return rc;
+    }
+    if (stats) *stats = st;
+    return SMCCAT_OK;
+}
+
+int smccat_smc_step(smccat_ctx* c, int32_t first, int32_t count, double* raw_weights,
+                    double target_ess, double last_temp, double* cur_temp, double* ess,
+                    double* norm_weights) {
+    if (!c || !raw_weights || !cur_temp || !ess || !norm_weights || count < 1 || first < 0)
+        return mfail(SMCCAT_EINVAL, "bad argument");
+    void* stv = nullptr;
+    int rc = smccat_get_stream(c, &stv);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stv);
+    // Scratch: the weights, normalised weights and two scalars, taken from a
+    // small device buffer owned by this call.
+    double* dbuf = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&dbuf, sizeof(double) * (2 * (size_t)count + 2), st);
+    if (e != cudaSuccess) return mfail(SMCCAT_ENOMEM, cudaGetErrorString(e));
+    const double* dlnl = lnl_device(c);
+    double out[2] = {0, 0};
+    if (!rc) {
+        e = cudaMemcpyAsync(dbuf, raw_weights, sizeof(double) * count, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) {
+            smc_step_kernel<<<1, kStepThreads, 0, st>>>(dbuf, dlnl + first, count, target_ess, last_temp,
+                                                        dbuf + count, dbuf + 2 * count);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(raw_weights, dbuf, sizeof(double) * count, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(norm_weights, dbuf + count, sizeof(double) * count, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out, dbuf + 2 * count, sizeof(out), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    cudaFreeAsync(dbuf, st);
+    if (rc) return rc;
+    if (e != cudaSuccess) return mfail(SMCCAT_ECUDA, cudaGetErrorString(e));
+    *cur_temp = out[0];
+    *ess = out[1];
+    return SMCCAT_OK;
+}
+
+}  // extern "C"

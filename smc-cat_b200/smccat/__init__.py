@@ -42,6 +42,23 @@ class Profile(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "adaptive_nni_epsilon", "shape_delta", "scale_delta", "subtree_scale_delta",
+        "stationary_delta", "rate_matrix_delta", "invar_alpha", "dpp_alpha")]
+
+
+class MoveStats(ctypes.Structure):
+    _fields_ = [("proposed", ctypes.c_uint64 * 10), ("accepted", ctypes.c_uint64 * 10),
+                ("lockstep_steps", ctypes.c_uint64)]
+
+
+MOVE_NAMES = ("Adaptive NNI", "NNI", "SPR", "Branch Length", "Scale Subtree",
+              "Proportion Invariant", "Rate Shape", "Stationary", "Rate Matrix Single",
+              "Rate Matrix Full")
+FAMILY_TREE, FAMILY_STATIONARY, FAMILY_SHAPE, FAMILY_INVAR, FAMILY_RATE_MATRIX = range(5)
+
+
 class Config(ctypes.Structure):
     _fields_ = [("num_taxa", _i32), ("num_sites", _i32), ("num_rates", _i32),
                 ("max_particles", _i32), ("max_classes", _i32), ("model_flags", _i32),
@@ -93,6 +110,17 @@ def lib():
         "smccat_get_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
         "smccat_set_profiling": ([vp, _i32], ctypes.c_int),
         "smccat_autotune": ([vp, _i32, _ip, _dp], ctypes.c_int),
+        "smccat_set_tuning": ([vp, ctypes.POINTER(Tuning)], ctypes.c_int),
+        "smccat_get_tuning": ([vp, ctypes.POINTER(Tuning)], ctypes.c_int),
+        "smccat_set_rate_cholesky": ([vp, _dp], ctypes.c_int),
+        "smccat_set_split_posteriors": ([vp, _i32, ctypes.POINTER(ctypes.c_uint64), _dp],
+                                        ctypes.c_int),
+        "smccat_ln_prior": ([vp, _i32, _i32, _dp], ctypes.c_int),
+        "smccat_propose": ([vp, _i32, _i32, ctypes.c_uint64, _ip, _dp], ctypes.c_int),
+        "smccat_rejuvenate": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64,
+                               ctypes.POINTER(MoveStats)], ctypes.c_int),
+        "smccat_smc_step": ([vp, _i32, _i32, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp,
+                             _dp], ctypes.c_int),
         "smccat_get_profile": ([vp, ctypes.POINTER(Profile)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -265,6 +293,59 @@ class Engine:
 
     def sync(self):
         _check(lib().smccat_sync(self._h))
+
+    # -- MCMC / SMC ---------------------------------------------------------
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(lib().smccat_get_tuning(self._h, ctypes.byref(t)))
+        return {n: getattr(t, n) for n, _ in Tuning._fields_}
+
+    def set_tuning(self, **kw):
+        cur = self.tuning()
+        cur.update(kw)
+        t = Tuning(**cur)
+        _check(lib().smccat_set_tuning(self._h, ctypes.byref(t)))
+
+    def set_rate_cholesky(self, L):
+        a, ap = _d(np.tril(np.asarray(L, dtype=np.float64)))
+        _check(lib().smccat_set_rate_cholesky(self._h, ap))
+
+    def set_split_posteriors(self, bits, probs):
+        b = np.ascontiguousarray(bits, dtype=np.uint64).reshape(-1, 2)
+        pr, prp = _d(probs)
+        _check(lib().smccat_set_split_posteriors(
+            self._h, len(pr), b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), prp))
+
+    def ln_prior(self, first=0, count=None) -> np.ndarray:
+        count = self.P - first if count is None else count
+        out = np.zeros(count)
+        _check(lib().smccat_ln_prior(self._h, int(first), int(count), out.ctypes.data_as(_dp)))
+        return out
+
+    def propose(self, p, family, seed):
+        k = ctypes.c_int32(-1)
+        h = ctypes.c_double(0.0)
+        _check(lib().smccat_propose(self._h, int(p), int(family), int(seed), ctypes.byref(k),
+                                    ctypes.byref(h)))
+        return int(k.value), float(h.value)
+
+    def rejuvenate(self, iterations, temperature, seed, first=0, count=None) -> dict:
+        count = self.P - first if count is None else count
+        st = MoveStats()
+        _check(lib().smccat_rejuvenate(self._h, int(first), int(count), int(iterations),
+                                       float(temperature), int(seed), ctypes.byref(st)))
+        return {"proposed": list(st.proposed), "accepted": list(st.accepted),
+                "lockstep_steps": int(st.lockstep_steps)}
+
+    def smc_step(self, raw_weights, target_ess, last_temp, first=0):
+        w = np.array(raw_weights, dtype=np.float64, copy=True)
+        nw = np.zeros_like(w)
+        t = ctypes.c_double(0.0)
+        e = ctypes.c_double(0.0)
+        _check(lib().smccat_smc_step(self._h, int(first), len(w), w.ctypes.data_as(_dp),
+                                     float(target_ess), float(last_temp), ctypes.byref(t),
+                                     ctypes.byref(e), nw.ctypes.data_as(_dp)))
+        return w, nw, e.value, t.value
 
     # -- measurement --------------------------------------------------------
     @property
