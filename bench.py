@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--particles", type=int, default=0,
                     help="override the particle count (small cases for ncu captures)")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--sweeps", type=int, default=2,
+                    help="timed rejuvenation sweeps (0 to skip)")
+    ap.add_argument("--sweep-temp", type=float, default=0.5)
     return ap.parse_args()
 
 
@@ -307,10 +310,27 @@ def main():
     prof_e2e = eng.profile()
     assert np.all(np.isfinite(lnl_host))
 
-    times = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+    # ---- rejuvenation sweeps: Mcmc::operator() x iterations on every particle -----
+    sweep_stats, ms_sweep = None, 0.0
+    if args.sweeps > 0:
+        load()
+        eng.refresh(full=True)
+        eng.rejuvenate(iterations=cfg.iterations, temperature=args.sweep_temp, seed=999 + rank)
+        barrier()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for k in range(args.sweeps):
+            sweep_stats = eng.rejuvenate(iterations=cfg.iterations, temperature=args.sweep_temp,
+                                         seed=1000 + k + 100 * rank)
+        s1.record(stream)
+        s1.synchronize()
+        barrier()
+        ms_sweep = s0.elapsed_time(s1)
+
+    times = torch.tensor([ms, ms_e2e, ms_sweep], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    ms, ms_e2e = times.tolist()
+    ms, ms_e2e, ms_sweep = times.tolist()
     total_units = units_per_step * args.steps * world
     value = total_units / (ms * 1e-3)
     e2e_value = None if args.skip_e2e else total_units / (ms_e2e * 1e-3)
@@ -356,6 +376,14 @@ def main():
                      "frac": (fp64_achieved / fp64_peak) if fp64_peak else None},
             "kernel_ms_per_step": {k: v / args.steps for k, v in prof["ms"].items()},
             "gpu_launches": sum(prof["launches"].values()),
+            "sweeps_per_s": (args.sweeps / (ms_sweep * 1e-3)) if args.sweeps > 0 else None,
+            "sweep": None if sweep_stats is None else {
+                "definition": f"Mcmc::operator() with {cfg.iterations} iterations on all {n} "
+                              f"particles per GPU at temperature {args.sweep_temp}, lockstep",
+                "ms_per_sweep": ms_sweep / args.sweeps,
+                "lockstep_steps": sweep_stats["lockstep_steps"],
+                "proposed": sum(sweep_stats["proposed"]),
+                "accepted": sum(sweep_stats["accepted"])},
             "clocks": clk,
         }
         if not args.no_cpu_baseline and world == 1:

@@ -277,6 +277,32 @@ int smccat_propose(smccat_ctx* ctx, int32_t p, int32_t family, uint64_t seed, in
 int smccat_rejuvenate(smccat_ctx* ctx, int32_t first, int32_t count, int32_t iterations,
                       double temperature, uint64_t seed, smccat_move_stats* stats);
 
+typedef struct smccat_gibbs_stats {
+    int64_t particles;       /* particles reassigned                         */
+    int64_t classes_before;  /* summed class counts before                   */
+    int64_t classes_after;   /* summed class counts after                    */
+    int64_t created;         /* classes created from auxiliary draws         */
+} smccat_gibbs_stats;
+
+/* Particle::gibbsPartitionMove(temperature) followed by refreshLikelihood(true)
+ * (Particle.cpp:785-995, main.cpp:303-306) for the particles of
+ * [first, first+count) whose mask byte is non-zero (mask may be NULL = all):
+ * Neal's Algorithm 8 with m = 5 auxiliary classes, floor(S/2) random-site
+ * iterations per particle, run on the device, one thread block per particle.
+ * Emptied classes are removed and the survivors renumbered in order; new
+ * classes are appended. Needs SMCCAT_MODEL_CAT and no pending edits; fails
+ * with SMCCAT_ENOMEM if a particle would exceed max_classes. */
+int smccat_gibbs(smccat_ctx* ctx, int32_t first, int32_t count, const uint8_t* mask,
+                 double temperature, uint64_t seed, smccat_gibbs_stats* stats);
+
+/* The unnormalised log weights one Gibbs iteration would draw from for site
+ * `site` of particle p, with the site taken out of its class and the 5
+ * auxiliary classes given as logits (5 x 20): K + 5 values, -inf for a class
+ * that the removal empties. Nothing is changed. Parity probe for
+ * Particle.cpp:857-941. */
+int smccat_gibbs_weights(smccat_ctx* ctx, int32_t p, int32_t site, const double* aux_logits,
+                         double temperature, double* out);
+
 /* computeNextStep (Miscellaneous.hpp:42-109) in FP64 on the device, on the
  * current log-likelihoods of [first, first+count): bisects the temperature
  * for `target_ess`, updates raw_weights in place and writes the normalised

@@ -688,6 +688,9 @@ const Slot& smccat::slot_of(const smccat_ctx* c, int p) { return c->slots[p]; }
 const Dims& smccat::dims_of(const smccat_ctx* c) { return c->d; }
 int smccat::model_flags_of(const smccat_ctx* c) { return c->cfg.model_flags; }
 const double* smccat::lnl_device(const smccat_ctx* c) { return c->d_lnl; }
+const uint8_t* smccat::codes_device(const smccat_ctx* c) { return c->d_codes; }
+const double* smccat::isinv_device(const smccat_ctx* c) { return c->d_isinv; }
+const int32_t* smccat::invchar_device(const smccat_ctx* c) { return c->d_invchar; }
 
 extern "C" {
 

@@ -49,6 +49,9 @@ const Slot& slot_of(const smccat_ctx* c, int p);
 const Dims& dims_of(const smccat_ctx* c);
 int model_flags_of(const smccat_ctx* c);
 const double* lnl_device(const smccat_ctx* c);  // [max_particles] current log-likelihoods
+const uint8_t* codes_device(const smccat_ctx* c);   // [T][S]
+const double* isinv_device(const smccat_ctx* c);    // [S]
+const int32_t* invchar_device(const smccat_ctx* c); // [S]
 
 // Drop the MCMC settings kept for a context (called by smccat_destroy).
 void mcmc_release(const smccat_ctx* c);

@@ -1,0 +1,302 @@
+// CAT class reassignment (Neal's Algorithm 8, m = 5 auxiliary classes) on the
+// device: Particle::gibbsPartitionMove (Particle.cpp:785-995), corrected form.
+//
+// One CTA per particle runs the floor(S/2) site iterations in order. Each
+// iteration: draw a site and take it out of its class (dropping the class if
+// it empties), draw m fresh classes from the prior (19 N(0,1) logits + 0,
+// TransitionProbabilityClass.cpp:26-35) and diagonalise them (one warp each),
+// evaluate the site's likelihood under every live class and every auxiliary
+// class (one warp per (class, rate) pair, lanes = states, single-site pruning
+// in the eigenbasis P(t)x = L (exp(lambda t) o (Rm x))), weight each class by
+// temperature * log L + log n_k (or log(alpha / m) for the auxiliaries) and
+// draw the new class. Random numbers come from a per-particle Philox stream.
+//
+// Two reference quirks are not reproduced: its tip read ignores the rate
+// stride (Particle.cpp:895) and its rescalers are written and read at
+// different strides (Particle.cpp:880 vs :921), so its weights mix in stale
+// buffer contents.
+#include <cuda_runtime.h>
+#include <curand_kernel.h>
+#include <math.h>
+
+#include "gibbs.h"
+#include "spectral.cuh"
+
+namespace smccat {
+namespace {
+
+constexpr int kGibbsWarps = 16;
+constexpr int kAux = 5;
+
+__device__ __forceinline__ double warp_max20(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// exp(lambda_m t_n r) for every (node, rate) of class slot k.
+__device__ void fill_exp(const GibbsArgs& a, int i, int k, const double* rec, double* ex) {
+    const Dims& d = a.d;
+    const GibbsPart& gp = a.parts[i];
+    const double* br = a.branch + (size_t)i * d.N;
+    for (int idx = threadIdx.x; idx < d.N * d.R * kStates; idx += blockDim.x) {
+        const int m = idx % kStates, r = (idx / kStates) % d.R, n = idx / (kStates * d.R);
+        ex[idx] = exp(rec[kSpecLam + m] * br[n] * gp.rates[r]);
+    }
+}
+
+// Log-likelihood of site s under class slot k and rate r, one warp.
+__device__ double site_rate_lnl(const GibbsArgs& a, int i, int s, int r, const double* rec,
+                                const double* ex, double* stash) {
+    const Dims& d = a.d;
+    const int lane = threadIdx.x & 31;
+    const int li = lane < kStates ? lane : 0;
+    double Lrow[kStates], Rrow[kStates];
+#pragma unroll
+    for (int m = 0; m < kStates; ++m) {
+        Lrow[m] = rec[kSpecL + li * kStates + m];   // L[lane][m]
+        Rrow[m] = rec[kSpecRm + li * kStates + m];  // Rm[lane][m]
+    }
+    double rs = 0.0;
+#pragma unroll
+    for (int j = 0; j < kStates; ++j) rs += Rrow[j];
+    const int32_t* tree = a.tree + (size_t)i * d.NI * 3;
+    double lsc = 0.0, v = 1.0;
+    for (int q = 0; q < d.NI; ++q) {
+        const int n = tree[3 * q];
+        v = 1.0;
+#pragma unroll 1
+        for (int ci = 1; ci <= 2; ++ci) {
+            const int c = tree[3 * q + ci];
+            const double e = ex[((size_t)c * d.R + r) * kStates + li];
+            double z;  // lane m: exp(lambda_m t) * (Rm x)_m
+            if (c < d.T) {
+                const int code = a.codes[(size_t)c * d.S + s];
+                double rc = rs;
+                if (code < kStates) {
+#pragma unroll
+                    for (int j = 0; j < kStates; ++j) rc = (j == code) ? Rrow[j] : rc;
+                }
+                z = e * rc;
+            } else {
+                const double xv = stash[(size_t)(c - d.T) * 32 + lane];
+                double acc = 0.0;
+#pragma unroll
+                for (int j = 0; j < kStates; ++j) acc = fma(Rrow[j], __shfl_sync(0xffffffffu, xv, j), acc);
+                z = e * acc;
+            }
+            double y = 0.0;
+#pragma unroll
+            for (int m = 0; m < kStates; ++m) y = fma(Lrow[m], __shfl_sync(0xffffffffu, z, m), y);
+            v *= y;
+        }
+        if (lane >= kStates) v = 0.0;
+        const double mx = warp_max20(v);
+        if (mx > 0.0) {
+            int e;
+            frexp(mx, &e);
+            v *= ldexp(1.0, -e);
+            lsc += e * 0.69314718055994530942;
+        } else {
+            lsc = -INFINITY;
+        }
+        stash[(size_t)(n - d.T) * 32 + lane] = v;
+        __syncwarp();
+    }
+    const double pi = (lane < kStates) ? rec[kSpecPi + lane] : 0.0;
+    const double sv = wsum(pi * v);
+    return log(sv) + lsc;
+}
+
+__global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
+    const Dims& d = a.d;
+    const int i = blockIdx.x;
+    const GibbsPart gp = a.parts[i];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int Kcap = a.Kcap;
+    double* spec = a.spec + (size_t)i * (Kcap + kAux) * kSpecStride;
+    double* ex = a.expt + (size_t)i * (Kcap + kAux) * d.N * d.R * kStates;
+    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * d.NI * 32;
+    double* logits = a.logits + (size_t)i * (Kcap + kAux) * kStates;
+    int32_t* assign = a.assign + (size_t)i * d.S;
+    const double* base = a.base + (size_t)i * kBase;
+    extern __shared__ double sh[];                   // lnl [(Kcap + kAux) * R]
+    double* wts = sh + (size_t)(Kcap + kAux) * d.R;  // [Kcap + kAux]
+    int* counts = reinterpret_cast<int*>(wts + (Kcap + kAux));  // [Kcap + kAux]
+    const bool weights_mode = gp.fixed_site >= 0;
+    __shared__ int s_site, s_kcur, s_choice;
+    __shared__ SpecWork work[kAux];
+    __shared__ curandStatePhilox4_32_10_t rng_state;
+
+    if (threadIdx.x == 0) {
+        curand_init(a.seed, (unsigned long long)gp.p, 0ull, &rng_state);
+        s_kcur = gp.K;
+    }
+    for (int k = threadIdx.x; k < Kcap + kAux; k += blockDim.x) counts[k] = 0;
+    __syncthreads();
+    for (int x = threadIdx.x; x < d.S; x += blockDim.x) atomicAdd(&counts[assign[x]], 1);
+    if (warp < kAux)  // one shared workspace per decomposing warp
+        for (int k = warp; k < gp.K; k += kAux)
+            spectral_decompose_warp_ws(base, logits + (size_t)k * kStates,
+                                       spec + (size_t)k * kSpecStride, work[warp]);
+    __syncthreads();
+    for (int k = 0; k < gp.K; ++k)
+        fill_exp(a, i, k, spec + (size_t)k * kSpecStride, ex + (size_t)k * d.N * d.R * kStates);
+    __syncthreads();
+
+    const double alpha_split = log(a.alpha / kAux);
+    for (int it = 0; it < gp.n_iter; ++it) {
+        // 1. draw the site and remove it from its class (Particle.cpp:808-821)
+        if (threadIdx.x == 0) {
+            int s;
+            if (weights_mode) {
+                s = gp.fixed_site;
+            } else {
+                const double u = curand_uniform_double(&rng_state);  // (0, 1]
+                s = (int)((1.0 - u) * d.S);
+                s = s < d.S ? s : d.S - 1;
+            }
+            s_site = s;
+            counts[assign[s]]--;
+            for (int j = 0; j < kAux; ++j)
+                for (int m = 0; m < kStates; ++m)
+                    logits[(size_t)(s_kcur + j) * kStates + m] =
+                        weights_mode ? a.aux_in[((size_t)i * kAux + j) * kStates + m]
+                                     : ((m < kStates - 1) ? curand_normal_double(&rng_state) : 0.0);
+        }
+        __syncthreads();
+        const int s = s_site, kcur = s_kcur;
+        // 2. diagonalise the auxiliary classes (Particle.cpp:823-833)
+        if (warp < kAux)
+            spectral_decompose_warp_ws(base, logits + (size_t)(kcur + warp) * kStates,
+                                       spec + (size_t)(kcur + warp) * kSpecStride, work[warp]);
+        __syncthreads();
+        for (int j = 0; j < kAux; ++j)
+            fill_exp(a, i, kcur + j, spec + (size_t)(kcur + j) * kSpecStride,
+                     ex + (size_t)(kcur + j) * d.N * d.R * kStates);
+        __syncthreads();
+        // 3. site log-likelihood per (class, rate) (Particle.cpp:857-930)
+        const int npairs = (kcur + kAux) * d.R;
+        for (int pr = warp; pr < npairs; pr += kGibbsWarps) {
+            const int k = pr / d.R, r = pr % d.R;
+            double l = -INFINITY;
+            if (k >= kcur || counts[k] > 0)
+                l = site_rate_lnl(a, i, s, r, spec + (size_t)k * kSpecStride,
+                                  ex + (size_t)k * d.N * d.R * kStates, stash);
+            if (lane == 0) sh[pr] = l;
+        }
+        __syncthreads();
+        // 4. weights and the draw (Particle.cpp:931-978)
+        if (threadIdx.x == 0) {
+            double wmax = -INFINITY;
+            for (int k = 0; k < kcur + kAux; ++k) {
+                double w = -INFINITY;
+                if (k >= kcur || counts[k] > 0) {
+                    double mx = -INFINITY;
+                    for (int r = 0; r < d.R; ++r) mx = fmax(mx, sh[k * d.R + r]);
+                    double lse = mx;
+                    if (mx > -INFINITY) {
+                        double se = 0.0;
+                        for (int r = 0; r < d.R; ++r) se += exp(sh[k * d.R + r] - mx);
+                        lse = mx + log(se);
+                    }
+                    const double* pi = spec + (size_t)k * kSpecStride + kSpecPi;
+                    double ls;
+                    if (gp.pinv > 0.0 && a.isinv[s] != 0) {
+                        const double la = log1p(-gp.pinv) + lse;
+                        const double lb = log(gp.pinv * pi[a.invchar[s]]);
+                        const double m2 = fmax(la, lb);
+                        ls = m2 + log(exp(la - m2) + exp(lb - m2));
+                    } else {
+                        ls = lse + log1p(-gp.pinv);
+                    }
+                    w = ls * a.temp + ((k < kcur) ? log((double)counts[k]) : alpha_split);
+                }
+                wts[k] = w;
+                wmax = fmax(wmax, w);
+            }
+            if (weights_mode) {
+                for (int k = 0; k < kcur + kAux; ++k)
+                    a.weights_out[(size_t)i * (Kcap + kAux) + k] = wts[k];
+                counts[assign[s]]++;  // leave the state as it was
+            }
+            double tot = 0.0;
+            for (int k = 0; k < kcur + kAux; ++k) tot += exp(wts[k] - wmax);
+            const double draw = tot * curand_uniform_double(&rng_state);
+            double run = 0.0;
+            int choice = kcur + kAux - 1;
+            for (int k = 0; k < kcur + kAux; ++k) {
+                const double w = wts[k];
+                if (w == -INFINITY) continue;
+                run += exp(w - wmax);
+                if (run >= draw) { choice = k; break; }
+            }
+            if (choice >= kcur && kcur >= Kcap) {
+                atomicOr(a.status, 4);  // class capacity exhausted: keep the old class
+                choice = assign[s];
+            }
+            if (weights_mode) choice = -1;
+            s_choice = choice;
+        }
+        __syncthreads();
+        const int choice = s_choice;
+        if (choice < 0) break;  // weights mode: nothing changes
+        if (choice >= kcur) {
+            // The chosen auxiliary becomes class slot kcur.
+            const int src = choice;
+            if (src != kcur) {
+                for (int x = threadIdx.x; x < kSpecStride; x += blockDim.x)
+                    spec[(size_t)kcur * kSpecStride + x] = spec[(size_t)src * kSpecStride + x];
+                for (int x = threadIdx.x; x < kStates; x += blockDim.x)
+                    logits[(size_t)kcur * kStates + x] = logits[(size_t)src * kStates + x];
+                for (int x = threadIdx.x; x < d.N * d.R * kStates; x += blockDim.x)
+                    ex[(size_t)kcur * d.N * d.R * kStates + x] = ex[(size_t)src * d.N * d.R * kStates + x];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                assign[s] = kcur;
+                counts[kcur] = 1;
+                s_kcur = kcur + 1;
+            }
+        } else if (threadIdx.x == 0) {
+            assign[s] = choice;
+            counts[choice]++;
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < s_kcur; k += blockDim.x) a.counts[(size_t)i * (Kcap + kAux) + k] = counts[k];
+    if (threadIdx.x == 0) a.kout[i] = s_kcur;
+}
+
+}  // namespace
+
+size_t gibbs_scratch_doubles(const Dims& d, int count, int Kcap) {
+    const size_t spec = (size_t)count * (Kcap + kAux) * kSpecStride;
+    const size_t ex = (size_t)count * (Kcap + kAux) * d.N * d.R * kStates;
+    const size_t stash = (size_t)count * kGibbsWarps * d.NI * 32;
+    return spec + ex + stash;
+}
+
+int gibbs_aux() { return kAux; }
+
+cudaError_t launch_gibbs(GibbsArgs a, double* scratch, cudaStream_t st) {
+    const Dims& d = a.d;
+    a.spec = scratch;
+    a.expt = a.spec + (size_t)a.count * (a.Kcap + kAux) * kSpecStride;
+    a.stash = a.expt + (size_t)a.count * (a.Kcap + kAux) * d.N * d.R * kStates;
+    const size_t smem = sizeof(double) * (size_t)(a.Kcap + kAux) * (d.R + 1) +
+                        sizeof(int) * (a.Kcap + kAux) + 16;
+    cudaError_t e = cudaFuncSetAttribute(gibbs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    gibbs_kernel<<<a.count, 32 * kGibbsWarps, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace smccat

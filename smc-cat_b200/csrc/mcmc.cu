@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "engine_internal.h"
+#include "gibbs.h"
 #include "host_math.h"
 #include "smccat.h"
 
@@ -583,6 +584,190 @@ int smccat_rejuvenate(smccat_ctx* c, int32_t first, int32_t count, int32_t itera
     }
     if (stats) *stats = st;
     return SMCCAT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Runs the device Gibbs kernel on the listed particles. In weights mode
+// (site >= 0) only writes the weight vector of particle list[0] and changes
+// nothing; otherwise installs the new class sets and refreshes.
+int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, uint64_t seed,
+              int site, const double* aux, double* weights_out, smccat_gibbs_stats* stats) {
+    const Dims& d = dims_of(c);
+    const int n = (int)list.size();
+    if (n == 0) return SMCCAT_OK;
+    const int naux = gibbs_aux();
+    const int Kcap = d.Kmax + 64;
+    const int ks = Kcap + naux;
+    std::vector<GibbsPart> parts(n);
+    std::vector<int32_t> tree((size_t)n * d.NI * 3), assign((size_t)n * d.S);
+    std::vector<double> branch((size_t)n * d.N), base((size_t)n * kBase), logits((size_t)n * ks * kStates, 0.0);
+    std::vector<double> auxv((size_t)n * naux * kStates, 0.0);
+    for (int j = 0; j < n; ++j) {
+        const Slot& s = slot_of(c, list[j]);
+        const Mirror& m = s.cur;
+        GibbsPart& g = parts[j];
+        g.p = list[j];
+        g.K = m.K;
+        g.n_iter = site >= 0 ? 1 : d.S / 2;  // Particle.cpp:791
+        g.fixed_site = site;
+        g.pinv = m.pinv;
+        for (int r = 0; r < kMaxRates; ++r) g.rates[r] = m.rates[r];
+        for (int q = 0; q < d.NI; ++q) {
+            const int x = m.post[q];
+            tree[((size_t)j * d.NI + q) * 3 + 0] = x;
+            tree[((size_t)j * d.NI + q) * 3 + 1] = m.kids[2 * x];
+            tree[((size_t)j * d.NI + q) * 3 + 2] = m.kids[2 * x + 1];
+        }
+        std::copy(m.branch.begin(), m.branch.end(), branch.begin() + (size_t)j * d.N);
+        std::copy(m.base.begin(), m.base.end(), base.begin() + (size_t)j * kBase);
+        std::copy(m.logits.begin(), m.logits.begin() + (size_t)m.K * kStates,
+                  logits.begin() + (size_t)j * ks * kStates);
+        std::copy(s.assign.begin(), s.assign.end(), assign.begin() + (size_t)j * d.S);
+        if (aux) std::copy(aux, aux + naux * kStates, auxv.begin() + (size_t)j * naux * kStates);
+    }
+    void* stv = nullptr;
+    int rc = smccat_get_stream(c, &stv);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stv);
+    // Device buffers for this call (inputs, outputs and kernel scratch).
+    const size_t scratch = gibbs_scratch_doubles(d, n, Kcap);
+    size_t bytes = 0;
+    auto carve = [&](size_t b) { const size_t o = bytes; bytes += (b + 255) & ~size_t(255); return o; };
+    const size_t o_parts = carve(sizeof(GibbsPart) * n), o_tree = carve(tree.size() * 4),
+                 o_branch = carve(branch.size() * 8), o_base = carve(base.size() * 8),
+                 o_logits = carve(logits.size() * 8), o_assign = carve(assign.size() * 4),
+                 o_counts = carve((size_t)n * ks * 4), o_kout = carve((size_t)n * 4),
+                 o_aux = carve(auxv.size() * 8), o_w = carve((size_t)n * ks * 8),
+                 o_status = carve(4), o_scr = carve(scratch * 8);
+    char* dbuf = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&dbuf, bytes, st);
+    if (e != cudaSuccess) return mfail(SMCCAT_ENOMEM, std::string("gibbs buffers: ") + cudaGetErrorString(e));
+    std::vector<int32_t> counts((size_t)n * ks), kout(n);
+    std::vector<double> wout((size_t)n * ks);
+    int status = 0;
+    auto up = [&](size_t o, const void* src, size_t b) {
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dbuf + o, src, b, cudaMemcpyHostToDevice, st);
+    };
+    auto down = [&](void* dst, size_t o, size_t b) {
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dst, dbuf + o, b, cudaMemcpyDeviceToHost, st);
+    };
+    up(o_parts, parts.data(), sizeof(GibbsPart) * n);
+    up(o_tree, tree.data(), tree.size() * 4);
+    up(o_branch, branch.data(), branch.size() * 8);
+    up(o_base, base.data(), base.size() * 8);
+    up(o_logits, logits.data(), logits.size() * 8);
+    up(o_assign, assign.data(), assign.size() * 4);
+    up(o_aux, auxv.data(), auxv.size() * 8);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dbuf + o_status, 0, 4, st);
+    if (e == cudaSuccess) {
+        GibbsArgs a{};
+        a.d = d;
+        a.count = n;
+        a.Kcap = Kcap;
+        a.temp = temperature;
+        a.alpha = tuning_of(c).t.dpp_alpha;
+        a.seed = seed;
+        a.parts = reinterpret_cast<const GibbsPart*>(dbuf + o_parts);
+        a.tree = reinterpret_cast<const int32_t*>(dbuf + o_tree);
+        a.branch = reinterpret_cast<const double*>(dbuf + o_branch);
+        a.base = reinterpret_cast<const double*>(dbuf + o_base);
+        a.logits = reinterpret_cast<double*>(dbuf + o_logits);
+        a.assign = reinterpret_cast<int32_t*>(dbuf + o_assign);
+        a.counts = reinterpret_cast<int32_t*>(dbuf + o_counts);
+        a.kout = reinterpret_cast<int32_t*>(dbuf + o_kout);
+        a.aux_in = aux ? reinterpret_cast<const double*>(dbuf + o_aux) : nullptr;
+        a.weights_out = reinterpret_cast<double*>(dbuf + o_w);
+        a.codes = codes_device(c);
+        a.isinv = isinv_device(c);
+        a.invchar = invchar_device(c);
+        a.status = reinterpret_cast<int*>(dbuf + o_status);
+        e = launch_gibbs(a, reinterpret_cast<double*>(dbuf + o_scr), st);
+    }
+    down(assign.data(), o_assign, assign.size() * 4);
+    down(counts.data(), o_counts, counts.size() * 4);
+    down(kout.data(), o_kout, kout.size() * 4);
+    down(logits.data(), o_logits, logits.size() * 8);
+    down(wout.data(), o_w, wout.size() * 8);
+    down(&status, o_status, 4);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFreeAsync(dbuf, st);
+    if (e != cudaSuccess) return mfail(SMCCAT_ECUDA, std::string("gibbs: ") + cudaGetErrorString(e));
+    if (site >= 0) {
+        const int K = slot_of(c, list[0]).cur.K;
+        for (int k = 0; k < K; ++k) weights_out[k] = wout[k];
+        for (int j = 0; j < naux; ++j) weights_out[K + j] = wout[K + j];
+        return SMCCAT_OK;
+    }
+    if (status & 4) return mfail(SMCCAT_ENOMEM, "Gibbs reassignment ran out of class slots");
+    // Compact the surviving classes and install the new assignments
+    // (the reference erases empty classes as it goes, Particle.cpp:817-821).
+    int first = *std::min_element(list.begin(), list.end());
+    int last = *std::max_element(list.begin(), list.end());
+    std::vector<uint8_t> act(last - first + 1, 0);
+    smccat_gibbs_stats gs{};
+    for (int j = 0; j < n; ++j) {
+        const int p = list[j];
+        const Slot& s = slot_of(c, p);
+        std::vector<int> remap(ks, -1);
+        int K = 0;
+        for (int k = 0; k < kout[j]; ++k)
+            if (counts[(size_t)j * ks + k] > 0) remap[k] = K++;
+        if (K > d.Kmax) return mfail(SMCCAT_ENOMEM, "Gibbs reassignment exceeded max_classes");
+        std::vector<double> nl((size_t)d.Kmax * kStates, 0.0);
+        for (int k = 0; k < kout[j]; ++k)
+            if (remap[k] >= 0)
+                std::copy(&logits[((size_t)j * ks + k) * kStates], &logits[((size_t)j * ks + k + 1) * kStates],
+                          nl.begin() + (size_t)remap[k] * kStates);
+        std::vector<int32_t> na(d.S);
+        for (int x = 0; x < d.S; ++x) na[x] = remap[assign[(size_t)j * d.S + x]];
+        gs.classes_before += s.cur.K;
+        gs.classes_after += K;
+        gs.created += std::max(0, kout[j] - s.cur.K);
+        const Mirror m = s.cur;  // copy: set_particles replaces the slot
+        const int32_t kk = K;
+        const double pv = m.pinv, sh = m.shape;
+        rc = smccat_set_particles(c, p, 1, m.parent.data(), m.branch.data(), m.base.data(), &kk,
+                                  nl.data(), na.data(), &pv, &sh);
+        if (rc) return rc;
+        act[p - first] = 1;
+    }
+    // refreshLikelihood(true) after the move (main.cpp:303-306).
+    rc = refresh_internal(c, first, last - first + 1, SMCCAT_REFRESH_FULL, act.data());
+    if (rc) return rc;
+    gs.particles = n;
+    if (stats) *stats = gs;
+    return SMCCAT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int smccat_gibbs(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* mask, double temperature,
+                 uint64_t seed, smccat_gibbs_stats* stats) {
+    if (!c || first < 0 || count < 0) return mfail(SMCCAT_EINVAL, "bad argument");
+    if (!(model_flags_of(c) & SMCCAT_MODEL_CAT)) return mfail(SMCCAT_EINVAL, "Gibbs reassignment needs SMCCAT_MODEL_CAT");
+    std::vector<int> list;
+    for (int i = 0; i < count; ++i) {
+        if (mask && !mask[i]) continue;
+        const Slot& s = slot_of(c, first + i);
+        if (!s.loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
+        if (s.pending) return mfail(SMCCAT_ESTATE, "particle has uncommitted edits");
+        list.push_back(first + i);
+    }
+    return run_gibbs(c, list, temperature, seed, -1, nullptr, nullptr, stats);
+}
+
+int smccat_gibbs_weights(smccat_ctx* c, int32_t p, int32_t site, const double* aux_logits,
+                         double temperature, double* out) {
+    if (!c || !aux_logits || !out || p < 0) return mfail(SMCCAT_EINVAL, "bad argument");
+    const Slot& s = slot_of(c, p);
+    if (!s.loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
+    if (site < 0 || site >= dims_of(c).S) return mfail(SMCCAT_EINVAL, "site out of range");
+    return run_gibbs(c, {p}, temperature, 0, site, aux_logits, out, nullptr);
 }
 
 int smccat_smc_step(smccat_ctx* c, int32_t first, int32_t count, double* raw_weights,

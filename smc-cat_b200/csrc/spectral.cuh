@@ -20,16 +20,30 @@ static __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Run by exactly one full warp; `rec` holds kSpecStride doubles.
-static __device__ __noinline__ void spectral_decompose_warp(const double* __restrict__ base,
-                                                     const double* __restrict__ logits,
-                                                     double* __restrict__ rec) {
-    const int lane = threadIdx.x;
-    __shared__ double A[kStates][kStates + 1];
-    __shared__ double V[kStates][kStates + 1];
-    __shared__ double pi[kStates], sq[kStates];
-    __shared__ double cs[10], sn[10];
-    __shared__ int pp[10], qq[10];
+// Shared-memory workspace of one decomposing warp.
+struct SpecWork {
+    double A[kStates][kStates + 1];
+    double V[kStates][kStates + 1];
+    double pi[kStates], sq[kStates];
+    double cs[10], sn[10];
+    int pp[10], qq[10];
+};
+
+// Run by exactly one full warp with its own workspace `w`; `rec` holds
+// kSpecStride doubles.
+static __device__ __noinline__ void spectral_decompose_warp_ws(const double* __restrict__ base,
+                                                               const double* __restrict__ logits,
+                                                               double* __restrict__ rec,
+                                                               SpecWork& w) {
+    const int lane = threadIdx.x & 31;
+    double(&A)[kStates][kStates + 1] = w.A;
+    double(&V)[kStates][kStates + 1] = w.V;
+    double(&pi)[kStates] = w.pi;
+    double(&sq)[kStates] = w.sq;
+    double(&cs)[10] = w.cs;
+    double(&sn)[10] = w.sn;
+    int(&pp)[10] = w.pp;
+    int(&qq)[10] = w.qq;
 
     double e = (lane < kStates) ? exp(logits[lane]) : 0.0;
     const double tot = warp_sum(e);
@@ -135,6 +149,14 @@ static __device__ __noinline__ void spectral_decompose_warp(const double* __rest
         rec[kSpecL + i * kStates + m] = V[i][m] / sq[i];   // L[i][m]
         rec[kSpecRm + m * kStates + i] = V[i][m] * sq[i];  // Rm[m][i]
     }
+}
+
+// For kernels whose blocks are a single decomposing warp.
+static __device__ __forceinline__ void spectral_decompose_warp(const double* __restrict__ base,
+                                                               const double* __restrict__ logits,
+                                                               double* __restrict__ rec) {
+    __shared__ SpecWork w;
+    spectral_decompose_warp_ws(base, logits, rec, w);
 }
 
 }  // namespace smccat

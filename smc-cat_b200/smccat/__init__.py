@@ -59,6 +59,11 @@ MOVE_NAMES = ("Adaptive NNI", "NNI", "SPR", "Branch Length", "Scale Subtree",
 FAMILY_TREE, FAMILY_STATIONARY, FAMILY_SHAPE, FAMILY_INVAR, FAMILY_RATE_MATRIX = range(5)
 
 
+class GibbsStats(ctypes.Structure):
+    _fields_ = [("particles", ctypes.c_int64), ("classes_before", ctypes.c_int64),
+                ("classes_after", ctypes.c_int64), ("created", ctypes.c_int64)]
+
+
 class Config(ctypes.Structure):
     _fields_ = [("num_taxa", _i32), ("num_sites", _i32), ("num_rates", _i32),
                 ("max_particles", _i32), ("max_classes", _i32), ("model_flags", _i32),
@@ -121,6 +126,9 @@ def lib():
                                ctypes.POINTER(MoveStats)], ctypes.c_int),
         "smccat_smc_step": ([vp, _i32, _i32, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp,
                              _dp], ctypes.c_int),
+        "smccat_gibbs": ([vp, _i32, _i32, _up, ctypes.c_double, ctypes.c_uint64,
+                          ctypes.POINTER(GibbsStats)], ctypes.c_int),
+        "smccat_gibbs_weights": ([vp, _i32, _i32, _dp, ctypes.c_double, _dp], ctypes.c_int),
         "smccat_get_profile": ([vp, ctypes.POINTER(Profile)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -336,6 +344,24 @@ class Engine:
                                        float(temperature), int(seed), ctypes.byref(st)))
         return {"proposed": list(st.proposed), "accepted": list(st.accepted),
                 "lockstep_steps": int(st.lockstep_steps)}
+
+    def gibbs(self, temperature, seed, mask=None, first=0, count=None) -> dict:
+        count = self.P - first if count is None else count
+        st = GibbsStats()
+        mp = None
+        if mask is not None:
+            m = np.ascontiguousarray(mask, dtype=np.uint8)
+            mp = m.ctypes.data_as(_up)
+        _check(lib().smccat_gibbs(self._h, int(first), int(count), mp, float(temperature),
+                                  int(seed), ctypes.byref(st)))
+        return {n: int(getattr(st, n)) for n, _ in GibbsStats._fields_}
+
+    def gibbs_weights(self, p, site, aux_logits, temperature, num_classes) -> np.ndarray:
+        aux, ap = _d(np.asarray(aux_logits, dtype=np.float64).reshape(5, 20))
+        out = np.zeros(int(num_classes) + 5)
+        _check(lib().smccat_gibbs_weights(self._h, int(p), int(site), ap, float(temperature),
+                                          out.ctypes.data_as(_dp)))
+        return out
 
     def smc_step(self, raw_weights, target_ess, last_temp, first=0):
         w = np.array(raw_weights, dtype=np.float64, copy=True)
