@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--sweeps", type=int, default=2,
                     help="timed rejuvenation sweeps (0 to skip)")
     ap.add_argument("--sweep-temp", type=float, default=0.5)
+    ap.add_argument("--mixed", type=int, default=1,
+                    help="also time the FP32 (mixed-precision) path on the same particles")
     return ap.parse_args()
 
 
@@ -327,10 +329,51 @@ def main():
         barrier()
         ms_sweep = s0.elapsed_time(s1)
 
-    times = torch.tensor([ms, ms_e2e, ms_sweep], dtype=torch.float64, device="cuda")
+    # ---- mixed precision (FP32 partials / matrices) on the same particles ----------
+    mixed, ms_mixed = None, 0.0
+    if args.mixed:
+        load()
+        eng.refresh(full=True)
+        ref64 = eng.lnl()
+        e32 = smccat.Engine(codes, cfg.R, n, max_classes=st["logits"].shape[1], lg=cfg.lg,
+                            invar=cfg.invar, cat=cfg.cat, device=local,
+                            precision=smccat.PREC_FP32)
+        e32.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                          st["logits"], st["assign"], st["pinv"], st["shape"])
+        e32.refresh(full=True)
+        tuned32 = e32.autotune(reps=2)
+        stream32 = torch.cuda.ExternalStream(e32.stream_ptr, device=torch.device("cuda", local))
+        for _ in range(args.warmup):
+            e32.refresh(full=True)
+        e32.set_profiling(True)
+        barrier()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream32)
+        for _ in range(args.steps):
+            e32.refresh(full=True)
+        m1.record(stream32)
+        m1.synchronize()
+        barrier()
+        ms_mixed = m0.elapsed_time(m1)
+        p32 = e32.profile()
+        dl = np.abs(e32.lnl() - ref64)
+        mixed = {"precision": "fp32 partials and matrices; fp64 eigensystems, log-scalers, sums",
+                 "ms_per_step": ms_mixed / args.steps,
+                 "prune_ms": p32["ms"]["prune"] / max(p32["launches"]["prune"], 1),
+                 "max_abs_dlogl_vs_fp64": float(dl.max()), "mean_abs_dlogl_vs_fp64": float(dl.mean()),
+                 "autotune": tuned32}
+        e32.close()
+
+    times = torch.tensor([ms, ms_e2e, ms_sweep, ms_mixed], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    ms, ms_e2e, ms_sweep = times.tolist()
+    ms, ms_e2e, ms_sweep, ms_mixed = times.tolist()
+    if mixed is not None:
+        mixed["value"] = units_per_step * args.steps * world / (ms_mixed * 1e-3)
+        mixed["unit"] = UNIT
+        b32 = (cfg.T - 1) * (20 * 4 + 8) + (cfg.T - 2) * (20 * 4 + 8) + cfg.T / cfg.R
+        mixed["roofline_hbm_frac"] = b32 * units_per_step / (mixed["prune_ms"] * 1e-3) / 1e9 / \
+            measured_peaks()[0]
     total_units = units_per_step * args.steps * world
     value = total_units / (ms * 1e-3)
     e2e_value = None if args.skip_e2e else total_units / (ms_e2e * 1e-3)
@@ -376,6 +419,7 @@ def main():
                      "frac": (fp64_achieved / fp64_peak) if fp64_peak else None},
             "kernel_ms_per_step": {k: v / args.steps for k, v in prof["ms"].items()},
             "gpu_launches": sum(prof["launches"].values()),
+            "mixed_precision": mixed,
             "sweeps_per_s": (args.sweeps / (ms_sweep * 1e-3)) if args.sweeps > 0 else None,
             "sweep": None if sweep_stats is None else {
                 "definition": f"Mcmc::operator() with {cfg.iterations} iterations on all {n} "

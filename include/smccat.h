@@ -48,6 +48,12 @@ extern "C" {
 
 /* precision */
 #define SMCCAT_PREC_FP64    0  /* plain FP64 pruning                         */
+#define SMCCAT_PREC_FP32    1  /* mixed: FP32 partials, transition matrices and
+                                  pruning arithmetic (the reference's
+                                  MIXED_PRECISION CL_TYPE = float,
+                                  Miscellaneous.hpp:13-17); eigensystems, the
+                                  exp(Lambda t) reconstruction, log-scalers and
+                                  the site / particle sums stay FP64          */
 
 /* refresh modes */
 #define SMCCAT_REFRESH_DIRTY 0 /* refreshLikelihood(false): dirty nodes only */

@@ -62,9 +62,10 @@ struct smccat_ctx {
     int32_t* d_perm = nullptr;
     Tile* d_tiles = nullptr;
     int32_t* d_tile_off = nullptr;
-    double* d_CL = nullptr;
+    unsigned char* d_CL = nullptr;   // partials, element size esz
     double* d_LSC = nullptr;
-    double* d_Pm = nullptr;
+    unsigned char* d_Pm = nullptr;   // transition matrices, element size esz
+    int esz = 8;                     // 8 (FP64) or 4 (mixed precision)
     double* d_spec = nullptr;
     uint8_t* d_sws = nullptr;
     double* d_partial = nullptr;
@@ -283,7 +284,8 @@ int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** o
     if (R < 1 || R > kMaxRates) return fail(SMCCAT_EINVAL, "num_rates must be in [1, 8]");
     if (cfg->max_particles < 1) return fail(SMCCAT_EINVAL, "max_particles must be >= 1");
     if (cfg->max_classes < 1 || cfg->max_classes > 4096) return fail(SMCCAT_EINVAL, "max_classes must be in [1, 4096]");
-    if (cfg->precision != SMCCAT_PREC_FP64) return fail(SMCCAT_EINVAL, "unsupported precision");
+    if (cfg->precision != SMCCAT_PREC_FP64 && cfg->precision != SMCCAT_PREC_FP32)
+        return fail(SMCCAT_EINVAL, "unsupported precision");
     for (size_t i = 0; i < (size_t)T * S; ++i)
         if (codes[i] > 22) return fail(SMCCAT_EINVAL, "alignment code > 22 at index " + std::to_string(i));
     int ndev = 0;
@@ -303,7 +305,8 @@ int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** o
     const size_t lsc = (size_t)P * d.NI * 2 * R * d.Spad;
     const size_t pm = (size_t)P * K * N * 2 * R * kPBlock;
     const size_t spec = (size_t)P * K * 2 * kSpecStride;
-    const size_t need = 8 * (cl + lsc + pm + spec);
+    const size_t esz = cfg->precision == SMCCAT_PREC_FP32 ? 4 : 8;
+    const size_t need = esz * (cl + pm) + 8 * (lsc + spec);
     cudaError_t e = cudaSetDevice(cfg->device);
     if (e != cudaSuccess) { delete c; return fail(SMCCAT_ECUDA, cudaGetErrorString(e)); }
     size_t free_b = 0, total_b = 0;
@@ -322,9 +325,10 @@ int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** o
     A(&c->d_perm, (size_t)P * S);
     A(&c->d_tiles, (size_t)c->tile_cap);
     A(&c->d_tile_off, (size_t)P + 1);
-    A(&c->d_CL, cl);
+    c->esz = (int)esz;
+    A(&c->d_CL, cl * esz);
     A(&c->d_LSC, lsc);
-    A(&c->d_Pm, pm);
+    A(&c->d_Pm, pm * esz);
     A(&c->d_spec, spec);
     A(&c->d_sws, (size_t)P * K);
     A(&c->d_partial, (size_t)c->tile_cap);
@@ -621,7 +625,7 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
     if (np_ > 0)
         CK(launch(c, SMCCAT_KERNEL_PMAT, [&] {
             return launch_pmat(reinterpret_cast<const PJob*>(c->d_plan + pjob_off), np_, d_hdr, first,
-                               c->d_sws, c->d_spec, c->d_Pm, d, c->st);
+                               c->d_sws, c->d_spec, c->d_Pm, c->esz == 4, d, c->st);
         }));
     PruneArgs a{};
     a.d = d;
@@ -638,6 +642,7 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
     a.isinv = c->d_isinv;
     a.invchar = c->d_invchar;
     a.CL = c->d_CL;
+    a.fp32 = c->esz == 4;
     a.LSC = c->d_LSC;
     a.site_lnl = c->d_site_lnl;
     a.partial = c->d_partial;
@@ -724,14 +729,18 @@ int smccat_get_transition_matrix(smccat_ctx* c, int32_t p, int32_t k, int32_t no
         r < 0 || r >= d.R)
         return fail(SMCCAT_EINVAL, "bad class / node / rate index");
     if (s.pending && !s.refreshed) return fail(SMCCAT_ESTATE, "particle has unrefreshed edits");
-    double blk[kPBlock];
+    unsigned char blk[kPBlock * 8];
     const size_t off = ((((size_t)p * d.Kmax + k) * d.N + node) * 2 + s.cur.pws[node]) *
                            (size_t)d.R * kPBlock + (size_t)r * kPBlock;
     CK(cudaSetDevice(c->cfg.device));
-    CK(d2h(c, blk, c->d_Pm + off, sizeof(blk)));
+    CK(d2h(c, blk, c->d_Pm + off * c->esz, (size_t)kPBlock * c->esz));
     CK(cudaStreamSynchronize(c->st));
     for (int i = 0; i < kStates; ++i)
-        for (int j = 0; j < kStates; ++j) out400[i * kStates + j] = blk[i * kPCols + j];
+        for (int j = 0; j < kStates; ++j) {
+            const size_t e = (size_t)i * kPCols + j;
+            out400[i * kStates + j] = c->esz == 4 ? (double)reinterpret_cast<const float*>(blk)[e]
+                                                  : reinterpret_cast<const double*>(blk)[e];
+        }
     return SMCCAT_OK;
 }
 

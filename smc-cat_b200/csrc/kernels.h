@@ -19,12 +19,14 @@ struct PruneArgs {
     const NodeJob* nodes;
     const uint8_t* codes;
     const int32_t* perm;
-    const double* Pm;
+    const void* Pm;   // double, or float when fp32
     const double* spec;
     const uint8_t* sws;
     const double* isinv;
     const int32_t* invchar;
-    double* CL;       // written and re-read inside one launch: never via the nc path
+    void* CL;         // double, or float when fp32; written and re-read inside one
+                      // launch, so never read through the non-coherent path
+    int fp32;         // mixed precision: FP32 partials and matrices
     double* LSC;
     double* site_lnl;
     double* partial;
@@ -33,7 +35,7 @@ struct PruneArgs {
 
 cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d, cudaStream_t st);
 cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, const uint8_t* sws,
-                        const double* spec, double* Pm, const Dims& d, cudaStream_t st);
+                        const double* spec, void* Pm, bool fp32, const Dims& d, cudaStream_t st);
 // Pruning kernel variants (register caps) available for R rate categories.
 int prune_variants(int R);
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);

@@ -28,7 +28,6 @@ namespace smccat {
 namespace {
 
 constexpr uint32_t kWaitLimit = 1u << 22;  // mbarrier polls before giving up
-constexpr uint32_t kPBytes = kPBlock * sizeof(double);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -81,15 +80,27 @@ __device__ __noinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
     return false;
 }
 
+template <class T> struct Pair;
+template <> struct Pair<double> { using type = double2; };
+template <> struct Pair<float> { using type = float2; };
+
+// Exact power-of-two rescale: returns the exponent e with mx = f 2^e, f in [0.5, 1).
+__device__ __forceinline__ int exponent_of(double mx) { int e; frexp(mx, &e); return e; }
+__device__ __forceinline__ int exponent_of(float mx) { int e; frexpf(mx, &e); return e; }
+__device__ __forceinline__ double pow2(double, int e) { return ldexp(1.0, e); }
+__device__ __forceinline__ float pow2(float, int e) { return ldexpf(1.0f, e); }
+
 // acc[i] = sum_j P[i][j] x[j] with P row-major (stride kPCols), broadcast reads.
-__device__ __forceinline__ void matvec(const double* __restrict__ P, const double* x, double* acc) {
+template <class T>
+__device__ __forceinline__ void matvec(const T* __restrict__ P, const T* x, T* acc) {
+    using P2 = typename Pair<T>::type;
 #pragma unroll
     for (int i = 0; i < kStates; ++i) {
-        const double2* row = reinterpret_cast<const double2*>(P + i * kPCols);
-        double s0 = 0.0, s1 = 0.0;
+        const P2* row = reinterpret_cast<const P2*>(P + i * kPCols);
+        T s0 = 0, s1 = 0;
 #pragma unroll
         for (int j = 0; j < kStates / 2; ++j) {
-            const double2 p2 = row[j];
+            const P2 p2 = row[j];
             s0 = fma(p2.x, x[2 * j], s0);
             s1 = fma(p2.y, x[2 * j + 1], s1);
         }
@@ -110,11 +121,13 @@ __global__ void __launch_bounds__(32) spec_kernel(const SpecJob* __restrict__ jo
 
 // ---------------------------------------------------------------------------
 // Transition matrices of one node for every class and rate.
+// Computed in FP64; stored as T (rounded once for the FP32 path).
+template <class T>
 __global__ void __launch_bounds__(128) pmat_kernel(const PJob* __restrict__ jobs,
                                                    const PartHdr* __restrict__ hdr, int first,
                                                    const uint8_t* __restrict__ sws,
                                                    const double* __restrict__ spec,
-                                                   double* __restrict__ Pm, Dims d) {
+                                                   T* __restrict__ Pm, Dims d) {
     const PJob job = jobs[blockIdx.x];
     const PartHdr* h = hdr + (job.p - first);
     __shared__ double L[kStates][kStates + 1];
@@ -141,8 +154,8 @@ __global__ void __launch_bounds__(128) pmat_kernel(const PJob* __restrict__ jobs
             rs[tid] = s;
         }
         __syncthreads();
-        double* out = Pm + ((((size_t)job.p * d.Kmax + k) * d.N + job.node) * 2 + job.pws) *
-                               (size_t)d.R * kPBlock;
+        T* out = Pm + ((((size_t)job.p * d.Kmax + k) * d.N + job.node) * 2 + job.pws) *
+                          (size_t)d.R * kPBlock;
         for (int idx = tid; idx < d.R * kPBlock; idx += blockDim.x) {
             const int r = idx / kPBlock, e = idx % kPBlock;
             const int i = e / kPCols, j = e % kPCols;
@@ -154,7 +167,7 @@ __global__ void __launch_bounds__(128) pmat_kernel(const PJob* __restrict__ jobs
 #pragma unroll
                 for (int m = 0; m < kStates; ++m) v = fma(L[i][m] * ex[r][m], rs[m], v);
             }
-            out[idx] = v;
+            out[idx] = static_cast<T>(v);
         }
     }
 }
@@ -163,7 +176,10 @@ __global__ void __launch_bounds__(128) pmat_kernel(const PJob* __restrict__ jobs
 // Pruning + root reduction of one tile: warp r handles rate category r.
 // MINB = CTAs per SM the register allocation must allow (the register cap is
 // 65536 / (32 R MINB)); the autotuner picks among the instantiated values.
-template <int R, int MINB>
+// T = storage and arithmetic type of partials and transition matrices
+// (double, or float for the mixed-precision path); log-scalers and the root
+// reduction are FP64 in both.
+template <class T, int R, int MINB>
 __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) {
     const Dims d = a.d;
     const int tile_id = a.tile_begin + blockIdx.x;
@@ -171,8 +187,10 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     const int p = tl.p;
     const PartHdr* h = a.hdr + (p - a.first);
     if (!h->active) return;  // uniform across the CTA
+    using P2 = typename Pair<T>::type;
+    constexpr uint32_t kPBytes = kPBlock * sizeof(T);
 
-    extern __shared__ __align__(128) double smem[];  // [R warps][2 buffers][2 children][kPBlock]
+    extern __shared__ __align__(128) unsigned char smem_raw[];  // [R warps][2 buffers][2 children][kPBlock]
     __shared__ __align__(8) uint64_t bars[R][2];
     __shared__ double red[R][32];
     __shared__ int bad;
@@ -181,17 +199,17 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     const bool valid = lane < tl.nslots;
     const int slot = tl.slot0 + (valid ? lane : 0);
     const int site = a.perm[(size_t)p * d.S + slot];
-    double* buf = smem + (size_t)r * 4 * kPBlock;
+    T* buf = reinterpret_cast<T*>(smem_raw) + (size_t)r * 4 * kPBlock;
 
     const size_t j_stride = (size_t)R * d.Spad;
     const size_t ws_stride = (size_t)kStates * j_stride;
     const size_t node_stride = 2 * ws_stride;
     const size_t lws_stride = j_stride;
-    double* CLp = a.CL + (size_t)p * d.NI * node_stride;
+    T* CLp = static_cast<T*>(a.CL) + (size_t)p * d.NI * node_stride;
     double* LSCp = a.LSC + (size_t)p * d.NI * 2 * lws_stride;
     const int col = r * d.Spad + slot;
-    const double* Pcls = a.Pm + ((size_t)p * d.Kmax + tl.k) * d.N * 2 * (size_t)R * kPBlock +
-                         (size_t)r * kPBlock;
+    const T* Pcls = static_cast<const T*>(a.Pm) +
+                    ((size_t)p * d.Kmax + tl.k) * d.N * 2 * (size_t)R * kPBlock + (size_t)r * kPBlock;
     auto pblock = [&](int child, int pws) {
         return Pcls + ((size_t)child * 2 + pws) * (size_t)R * kPBlock;
     };
@@ -213,7 +231,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
         tma_load_1d(buf + kPBlock, pblock(nj.c2, (nj.ws >> 4) & 1), kPBytes, &bars[r][0]);
     }
 
-    double y[kStates];
+    T y[kStates];
     double lsc = 0.0;
     int prev = -1;
     bool ok = true;
@@ -253,9 +271,9 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
         }
         phase ^= 1u << b;
         if (ok && valid) {
-            const double* Pf = buf + (size_t)(b * 2 + fi) * kPBlock;
-            const double* Po = buf + (size_t)(b * 2 + oi) * kPBlock;
-            double acc[kStates];
+            const T* Pf = buf + (size_t)(b * 2 + fi) * kPBlock;
+            const T* Po = buf + (size_t)(b * 2 + oi) * kPBlock;
+            T acc[kStates];
             double lsc_f = 0.0;
             if (c1prev || c2prev) {
                 matvec(Pf, y, acc);
@@ -266,7 +284,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
                 const int f = fi ? nj.c2 : nj.c1;
                 if (f >= d.T) {
                     const int wsf = (nj.ws >> (1 + fi)) & 1;
-                    const double* fp = CLp + (size_t)(f - d.T) * node_stride + wsf * ws_stride + col;
+                    const T* fp = CLp + (size_t)(f - d.T) * node_stride + wsf * ws_stride + col;
 #pragma unroll
                     for (int j = 0; j < kStates; ++j) y[j] = fp[j * j_stride];
                     lsc_f = LSCp[(size_t)(f - d.T) * 2 * lws_stride + wsf * lws_stride + col];
@@ -282,16 +300,16 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
                 // The register child is consumed; its registers now hold the
                 // other child's stored partial, folded in row by row.
                 const int wsc = (nj.ws >> (1 + oi)) & 1;
-                const double* xp = CLp + (size_t)(o - d.T) * node_stride + wsc * ws_stride + col;
+                const T* xp = CLp + (size_t)(o - d.T) * node_stride + wsc * ws_stride + col;
 #pragma unroll
                 for (int j = 0; j < kStates; ++j) y[j] = xp[j * j_stride];
 #pragma unroll
                 for (int i = 0; i < kStates; ++i) {
-                    const double2* row = reinterpret_cast<const double2*>(Po + i * kPCols);
-                    double s0 = 0.0, s1 = 0.0;
+                    const P2* row = reinterpret_cast<const P2*>(Po + i * kPCols);
+                    T s0 = 0, s1 = 0;
 #pragma unroll
                     for (int j = 0; j < kStates / 2; ++j) {
-                        const double2 p2 = row[j];
+                        const P2 p2 = row[j];
                         s0 = fma(p2.x, y[2 * j], s0);
                         s1 = fma(p2.y, y[2 * j + 1], s1);
                     }
@@ -302,23 +320,22 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
 #pragma unroll
                 for (int i = 0; i < kStates; ++i) acc[i] *= Po[i * kPCols + cc];
             }
-            double mx = 0.0;
+            T mx = 0;
 #pragma unroll
             for (int i = 0; i < kStates; ++i) mx = fmax(mx, acc[i]);
             double l;
-            if (mx > 0.0) {
-                int e;
-                frexp(mx, &e);
-                const double sc = ldexp(1.0, -e);
+            if (mx > 0) {
+                const int e = exponent_of(mx);
+                const T sc = pow2(mx, -e);
 #pragma unroll
                 for (int i = 0; i < kStates; ++i) acc[i] *= sc;
                 l = e * 0.69314718055994530942;
             } else {
-                l = (mx == 0.0) ? -INFINITY : NAN;
+                l = (mx == 0) ? -INFINITY : NAN;
             }
             lsc = l + lsc_f + lsc_o;
             const int wso = nj.ws & 1;
-            double* out = CLp + (size_t)(nj.node - d.T) * node_stride + wso * ws_stride + col;
+            T* out = CLp + (size_t)(nj.node - d.T) * node_stride + wso * ws_stride + col;
 #pragma unroll
             for (int j = 0; j < kStates; ++j) {
                 y[j] = acc[j];
@@ -339,7 +356,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     }
     // Root reduction for this tile.
     if (cnt == 0 && valid) {
-        const double* xp = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride + col;
+        const T* xp = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride + col;
 #pragma unroll
         for (int j = 0; j < kStates; ++j) y[j] = xp[j * j_stride];
         lsc = LSCp[(size_t)(h->root - d.T) * 2 * lws_stride + h->root_ws * lws_stride + col];
@@ -350,7 +367,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     if (valid) {
         double s = 0.0;
 #pragma unroll
-        for (int i = 0; i < kStates; ++i) s = fma(pi[i], y[i], s);
+        for (int i = 0; i < kStates; ++i) s = fma(pi[i], (double)y[i], s);
         red[r][lane] = log(s) + lsc;
     }
     __syncthreads();
@@ -414,22 +431,41 @@ cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d,
 }
 
 cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, const uint8_t* sws,
-                        const double* spec, double* Pm, const Dims& d, cudaStream_t st) {
+                        const double* spec, void* Pm, bool fp32, const Dims& d, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    pmat_kernel<<<n, 128, 0, st>>>(jobs, hdr, first, sws, spec, Pm, d);
+    if (fp32) pmat_kernel<float><<<n, 128, 0, st>>>(jobs, hdr, first, sws, spec, static_cast<float*>(Pm), d);
+    else pmat_kernel<double><<<n, 128, 0, st>>>(jobs, hdr, first, sws, spec, static_cast<double*>(Pm), d);
     return cudaGetLastError();
 }
 
 namespace {
 
-template <int R, int MINB>
+template <class T, int R, int MINB>
 cudaError_t launch_prune_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
-    const size_t smem = sizeof(double) * 4 * (size_t)kPBlock * R;
-    cudaError_t e = cudaFuncSetAttribute(prune_kernel<R, MINB>,
+    const size_t smem = sizeof(T) * 4 * (size_t)kPBlock * R;
+    cudaError_t e = cudaFuncSetAttribute(prune_kernel<T, R, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    prune_kernel<R, MINB><<<ntiles, 32 * R, smem, st>>>(a);
+    prune_kernel<T, R, MINB><<<ntiles, 32 * R, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_prune_typed(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
+    switch (a.d.R) {
+        case 1: return launch_prune_t<T, 1, 4>(a, ntiles, st);
+        case 2: return launch_prune_t<T, 2, 4>(a, ntiles, st);
+        case 3: return launch_prune_t<T, 3, 4>(a, ntiles, st);
+        case 4:
+            if (variant == 1) return launch_prune_t<T, 4, 3>(a, ntiles, st);
+            if (variant == 2) return launch_prune_t<T, 4, 2>(a, ntiles, st);
+            return launch_prune_t<T, 4, 4>(a, ntiles, st);
+        case 5: return launch_prune_t<T, 5, 2>(a, ntiles, st);
+        case 6: return launch_prune_t<T, 6, 2>(a, ntiles, st);
+        case 7: return launch_prune_t<T, 7, 2>(a, ntiles, st);
+        case 8: return launch_prune_t<T, 8, 2>(a, ntiles, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace
@@ -438,20 +474,8 @@ int prune_variants(int R) { return R == 4 ? 3 : 1; }
 
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
     if (ntiles <= 0) return cudaSuccess;
-    switch (a.d.R) {
-        case 1: return launch_prune_t<1, 4>(a, ntiles, st);
-        case 2: return launch_prune_t<2, 4>(a, ntiles, st);
-        case 3: return launch_prune_t<3, 4>(a, ntiles, st);
-        case 4:
-            if (variant == 1) return launch_prune_t<4, 3>(a, ntiles, st);
-            if (variant == 2) return launch_prune_t<4, 2>(a, ntiles, st);
-            return launch_prune_t<4, 4>(a, ntiles, st);
-        case 5: return launch_prune_t<5, 2>(a, ntiles, st);
-        case 6: return launch_prune_t<6, 2>(a, ntiles, st);
-        case 7: return launch_prune_t<7, 2>(a, ntiles, st);
-        case 8: return launch_prune_t<8, 2>(a, ntiles, st);
-        default: return cudaErrorInvalidValue;
-    }
+    return a.fp32 ? launch_prune_typed<float>(a, ntiles, variant, st)
+                  : launch_prune_typed<double>(a, ntiles, variant, st);
 }
 
 cudaError_t launch_reduce(const int32_t* tile_off, const double* partial, const PartHdr* hdr, int first,

@@ -19,7 +19,7 @@ HEADER_PATH = os.path.join(os.path.dirname(_PKG_DIR), "include", "smccat.h")
 
 OK, EINVAL, ECUDA, ENOMEM, ESTATE, ENUMERIC, ENODEV = range(7)
 MODEL_LG, MODEL_INVAR, MODEL_CAT = 1, 2, 4
-PREC_FP64 = 0
+PREC_FP64, PREC_FP32 = 0, 1
 REFRESH_DIRTY, REFRESH_FULL = 0, 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -178,7 +178,8 @@ class Engine:
     """
 
     def __init__(self, codes, num_rates: int, max_particles: int, max_classes: int = 1,
-                 lg: bool = False, invar: bool = False, cat: bool = False, device: int = 0):
+                 lg: bool = False, invar: bool = False, cat: bool = False, device: int = 0,
+                 precision: int = PREC_FP64):
         codes = np.ascontiguousarray(codes, dtype=np.uint8)
         self.T, self.S = codes.shape
         self.R = int(num_rates)
@@ -186,7 +187,8 @@ class Engine:
         self.P = int(max_particles)
         self.Kmax = int(max_classes)
         flags = (MODEL_LG if lg else 0) | (MODEL_INVAR if invar else 0) | (MODEL_CAT if cat else 0)
-        cfg = Config(self.T, self.S, self.R, self.P, self.Kmax, flags, PREC_FP64, device)
+        self.precision = int(precision)
+        cfg = Config(self.T, self.S, self.R, self.P, self.Kmax, flags, self.precision, device)
         h = ctypes.c_void_p()
         _check(lib().smccat_create(ctypes.byref(cfg), codes.ctypes.data_as(_up), ctypes.byref(h)))
         self._h = h

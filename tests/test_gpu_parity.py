@@ -265,6 +265,52 @@ def test_protocol_errors():
     eng.close()
 
 
+MIXED_ATOL = 1e-3  # |dlogL| per particle (nats) allowed for the FP32 path
+
+
+@pytest.mark.parametrize("cfg", SMALL, ids=lambda c: c.name)
+def test_mixed_precision_full_refresh(cfg):
+    rng = np.random.default_rng(cfg.seed)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    st = workload.make_particles(cfg, cfg.particles, rng)
+    eng = smccat.Engine(codes, cfg.R, cfg.particles, max_classes=st["logits"].shape[1],
+                        lg=cfg.lg, invar=cfg.invar, cat=cfg.cat, precision=smccat.PREC_FP32)
+    eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                      st["logits"], st["assign"], st["pinv"], st["shape"])
+    eng.refresh(full=True)
+    got = eng.lnl()
+    for i in range(cfg.particles):
+        ref, _ = oracle_lnl(codes, st, i, cfg.R)
+        assert abs(got[i] - ref) <= MIXED_ATOL, (i, got[i] - ref)
+    eng.close()
+
+
+def test_mixed_precision_dirty_edits():
+    cfg = SMALL[2]
+    rng = np.random.default_rng(5)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    st = workload.make_particles(cfg, 3, rng)
+    eng = smccat.Engine(codes, cfg.R, 3, max_classes=st["logits"].shape[1], invar=True, cat=True,
+                        precision=smccat.PREC_FP32)
+    eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                      st["logits"], st["assign"], st["pinv"], st["shape"])
+    eng.refresh(full=True)
+    cur = {k: v.copy() for k, v in st.items()}
+    for step in range(6):
+        for i in range(3):
+            x = int(rng.integers(0, 2 * cfg.T - 2))
+            x = x if cur["parent"][i][x] >= 0 else x + 1
+            cur["branch"][i, x] *= 1.5
+            eng.set_branch_lengths(i, [x], [cur["branch"][i, x]])
+        eng.refresh()
+        eng.accept(np.ones(3, np.uint8))
+        got = eng.lnl()
+        for i in range(3):
+            ref, _ = oracle_lnl(codes, cur, i, cfg.R)
+            assert abs(got[i] - ref) <= MIXED_ATOL
+    eng.close()
+
+
 @pytest.mark.parametrize("cid", [1, 2])
 def test_reference_configs_full_size(cid):
     """Configs 1 and 2 at full size: every particle against the oracle."""
