@@ -63,19 +63,22 @@ def parse():
     return ap.parse_args()
 
 
-def algorithmic_cost(T: int, R: int):
+def algorithmic_cost(T: int, R: int, w: int = 8):
     """Per (particle, site, category) unit of one full refresh, stored-CL design.
 
-    Bytes: each of the T-1 internal nodes writes its 20-state FP64 partial and
-    one FP64 cumulative log-scaler; each of the T-2 internal non-root nodes is
-    read back once by its parent (partial + scaler); each tip contributes its
-    1-byte code per site (shared by the R categories).
+    Bytes (the roofline's algorithmic figure): per internal node one 20-state
+    partial written, two child 20-state partials read and one scaler written,
+    B = (T-1) * (3 * 20 * w + 8) with w the partial's element width.
+    Also returned: the minimum HBM bytes of this engine's layout, where child
+    partials come back from L2 and tips are never stored -- the T-1 partial and
+    scaler writes, B_min = (T-1) * (20 * w + 8).
     Flops (the reference's count): two dense 20x20 child mat-vecs, the
-    Hadamard product and the rescale per internal node: (T-1) * 1660.
+    Hadamard product and the rescale per internal node, F = (T-1) * 1660.
     """
-    b = (T - 1) * (20 * 8 + 8) + (T - 2) * (20 * 8 + 8) + T / R
+    b = (T - 1) * (3 * 20 * w + 8)
+    b_min = (T - 1) * (20 * w + 8)
     f = (T - 1) * (2 * 800 + 60)
-    return b, f
+    return b, f, b_min
 
 
 class ClockSampler:
@@ -371,15 +374,17 @@ def main():
     if mixed is not None:
         mixed["value"] = units_per_step * args.steps * world / (ms_mixed * 1e-3)
         mixed["unit"] = UNIT
-        b32 = (cfg.T - 1) * (20 * 4 + 8) + (cfg.T - 2) * (20 * 4 + 8) + cfg.T / cfg.R
+        b32, _, b32_min = algorithmic_cost(cfg.T, cfg.R, w=4)
         mixed["roofline_hbm_frac"] = b32 * units_per_step / (mixed["prune_ms"] * 1e-3) / 1e9 / \
             measured_peaks()[0]
+        mixed["min_bytes_hbm_frac"] = b32_min * units_per_step / (mixed["prune_ms"] * 1e-3) / \
+            1e9 / measured_peaks()[0]
     total_units = units_per_step * args.steps * world
     value = total_units / (ms * 1e-3)
     e2e_value = None if args.skip_e2e else total_units / (ms_e2e * 1e-3)
 
     if rank == 0:
-        b_unit, f_unit = algorithmic_cost(cfg.T, cfg.R)
+        b_unit, f_unit, b_min = algorithmic_cost(cfg.T, cfg.R)
         prune_ms = prof["ms"]["prune"] / max(prof["launches"]["prune"], 1)
         bytes_per_launch = b_unit * units_per_step
         achieved = bytes_per_launch / (prune_ms * 1e-3) / 1e9
@@ -390,7 +395,8 @@ def main():
             with open(tpath) as f:
                 tj = json.load(f)
             if tj.get("workload") == cfg.name:
-                traffic = tj.get("dram_bytes_per_launch")
+                # measured on a small case; DRAM bytes scale with the units processed
+                traffic = tj["dram_bytes"] / tj["units"] * units_per_step
         try:
             fp64_peak = dgemm_peak_tflops()
         except Exception:
@@ -414,6 +420,9 @@ def main():
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "prune_kernel<4>", "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "algorithmic_bytes_per_unit": b_unit,
+                         "min_bytes_per_unit": b_min,
+                         "min_bytes_frac": b_min * units_per_step / (prune_ms * 1e-3) / 1e9 / peak,
                          "avg_launch_ms": prune_ms},
             "fp64": {"achieved_tflops": fp64_achieved, "dgemm_peak_tflops": fp64_peak,
                      "frac": (fp64_achieved / fp64_peak) if fp64_peak else None},
