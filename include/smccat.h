@@ -309,6 +309,49 @@ int smccat_gibbs(smccat_ctx* ctx, int32_t first, int32_t count, const uint8_t* m
 int smccat_gibbs_weights(smccat_ctx* ctx, int32_t p, int32_t site, const double* aux_logits,
                          double temperature, double* out);
 
+/* ---- learned CAT class proposal (no reference counterpart: the reference's
+ * only reassignment move is the Gibbs sweep above) ----------------------- */
+
+/* Parameter count of the scoring MLP: 44 inputs, two ReLU layers of 128,
+ * one linear output; layout W1[44][128], b1, W2[128][128], b2, w3[128], b3. */
+#define SMCCAT_MLP_PARAMS 22401
+#define SMCCAT_MLP_INPUTS 44
+
+/* Train the scoring MLP (FP32, Adam) on the class assignments of particles
+ * [first, first+count) -- the samples plain Gibbs reassignment produces during
+ * warm-up -- for `epochs` passes in batches of `batch_sites` sites. The first
+ * call initialises the weights (Glorot, seeded). Writes the last epoch's mean
+ * softmax cross-entropy. Needs SMCCAT_MODEL_CAT. */
+int smccat_learned_train(smccat_ctx* ctx, int32_t first, int32_t count, int32_t epochs,
+                         int32_t batch_sites, double lr, uint64_t seed, double* loss_out);
+
+/* Mean softmax cross-entropy and its gradient for a given batch: n_sites
+ * groups, group g owning feature rows [group_off[g], group_off[g+1]) of x
+ * (rows of SMCCAT_MLP_INPUTS floats) with the correct row labels[g] (relative
+ * to the group). Uses the current parameters; changes nothing. */
+int smccat_learned_gradients(smccat_ctx* ctx, int32_t n_sites, const int32_t* group_off,
+                             const float* x, const int32_t* labels, float* grad_out,
+                             double* loss_out);
+
+/* Read (get_out) and/or replace (set_in) the SMCCAT_MLP_PARAMS parameters. */
+int smccat_learned_params(smccat_ctx* ctx, float* get_out, const float* set_in);
+
+typedef struct smccat_learned_stats {
+    int64_t proposed;
+    int64_t accepted;
+} smccat_learned_stats;
+
+/* Metropolis-Hastings class reassignment with the learned proposal for the
+ * masked particles of [first, first+count): `updates` random-site updates per
+ * particle; each proposes a class from the softmax of the MLP scores (BF16
+ * weights, FP32 arithmetic) among the existing classes and accepts with the
+ * tempered likelihood ratio, the CRP prior ratio n_b / (n_a - 1) and the
+ * proposal ratio, so the posterior is unchanged. Sites whose class would empty
+ * are not moved. Then refreshLikelihood(true). */
+int smccat_learned_move(smccat_ctx* ctx, int32_t first, int32_t count, const uint8_t* mask,
+                        int32_t updates, double temperature, uint64_t seed,
+                        smccat_learned_stats* stats);
+
 /* computeNextStep (Miscellaneous.hpp:42-109) in FP64 on the device, on the
  * current log-likelihoods of [first, first+count): bisects the temperature
  * for `target_ess`, updates raw_weights in place and writes the normalised

@@ -259,6 +259,7 @@ int smccat_lg_exchangeabilities(double* out190) {
 int smccat_destroy(smccat_ctx* c) {
     if (!c) return SMCCAT_OK;
     mcmc_release(c);
+    learned_release(c);
     cudaSetDevice(c->cfg.device);
     if (c->st) cudaStreamSynchronize(c->st);
     void* dptrs[] = {c->d_codes, c->d_isinv, c->d_invchar, c->d_perm, c->d_tiles, c->d_tile_off,
@@ -694,6 +695,7 @@ const Dims& smccat::dims_of(const smccat_ctx* c) { return c->d; }
 int smccat::model_flags_of(const smccat_ctx* c) { return c->cfg.model_flags; }
 const double* smccat::lnl_device(const smccat_ctx* c) { return c->d_lnl; }
 const uint8_t* smccat::codes_device(const smccat_ctx* c) { return c->d_codes; }
+const uint8_t* smccat::codes_host(const smccat_ctx* c) { return c->codes.data(); }
 const double* smccat::isinv_device(const smccat_ctx* c) { return c->d_isinv; }
 const int32_t* smccat::invchar_device(const smccat_ctx* c) { return c->d_invchar; }
 

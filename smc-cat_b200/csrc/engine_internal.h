@@ -53,7 +53,13 @@ const uint8_t* codes_device(const smccat_ctx* c);   // [T][S]
 const double* isinv_device(const smccat_ctx* c);    // [S]
 const int32_t* invchar_device(const smccat_ctx* c); // [S]
 
+const uint8_t* codes_host(const smccat_ctx* c);     // [T][S]
+
 // Drop the MCMC settings kept for a context (called by smccat_destroy).
 void mcmc_release(const smccat_ctx* c);
+// Drop the learned proposal kept for a context (called by smccat_destroy).
+void learned_release(const smccat_ctx* c);
+// BF16 MLP parameters and the device site features, or null if untrained.
+const void* learned_inference_weights(const smccat_ctx* c, const float** site_feat);
 
 }  // namespace smccat

@@ -20,6 +20,8 @@
 #include <math.h>
 
 #include "gibbs.h"
+#include "learned.h"
+#include <cuda_bf16.h>
 #include "spectral.cuh"
 
 namespace smccat {
@@ -274,7 +276,230 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
     if (threadIdx.x == 0) a.kout[i] = s_kcur;
 }
 
+// ---------------------------------------------------------------------------
+// Learned-proposal site reassignment.
+
+// Score of one (site, class) feature row x (kMlpIn floats, shared) by one warp;
+// W is the BF16 parameter vector in shared memory, h a 128-float warp buffer.
+__device__ float mlp_score(const __nv_bfloat16* W, const float* x, float* h) {
+    const int lane = threadIdx.x & 31;
+    float h1[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = lane + 32 * q;
+        float v = __bfloat162float(W[kMlpB1 + j]);
+        for (int i = 0; i < kMlpIn; ++i) v = fmaf(x[i], __bfloat162float(W[kMlpW1 + i * kMlpHid + j]), v);
+        h1[q] = fmaxf(v, 0.f);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) h[lane + 32 * q] = h1[q];
+    __syncwarp();
+    float part = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = lane + 32 * q;
+        float v = __bfloat162float(W[kMlpB2 + j]);
+        for (int i = 0; i < kMlpHid; ++i) v = fmaf(h[i], __bfloat162float(W[kMlpW2 + i * kMlpHid + j]), v);
+        part = fmaf(fmaxf(v, 0.f), __bfloat162float(W[kMlpW3 + j]), part);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    return part + __bfloat162float(W[kMlpB3]);
+}
+
+// Feature row of (site features sf, class stationary pi, class size n) by one warp.
+__device__ void mlp_features(const float* sf, const double* pi, int n, float* x) {
+    const int lane = threadIdx.x & 31;
+    if (lane < kSiteFeat) x[lane] = sf[lane];
+    if (lane < kStates) x[kSiteFeat + lane] = (float)pi[lane];
+    double dot = (lane < kStates) ? sf[lane] * log(pi[lane]) : 0.0;
+    dot = wsum(dot);
+    if (lane == 0) {
+        x[kSiteFeat + 20] = logf((float)(n > 1 ? n : 1));
+        x[kSiteFeat + 21] = (float)dot;
+        x[kSiteFeat + 22] = 0.f;
+    }
+    __syncwarp();
+}
+
+// Tempered, +I-mixed site log-likelihood from per-rate values l[r].
+__device__ double site_value(const GibbsArgs& a, const GibbsPart& gp, int s, const double* l,
+                             const double* pi) {
+    double mx = -INFINITY;
+    for (int r = 0; r < a.d.R; ++r) mx = fmax(mx, l[r]);
+    double lse = mx;
+    if (mx > -INFINITY) {
+        double se = 0.0;
+        for (int r = 0; r < a.d.R; ++r) se += exp(l[r] - mx);
+        lse = mx + log(se);
+    }
+    if (gp.pinv > 0.0 && a.isinv[s] != 0) {
+        const double la = log1p(-gp.pinv) + lse;
+        const double lb = log(gp.pinv * pi[a.invchar[s]]);
+        const double m2 = fmax(la, lb);
+        return m2 + log(exp(la - m2) + exp(lb - m2));
+    }
+    return lse + log1p(-gp.pinv);
+}
+
+__global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArgs a,
+                                                                        const __nv_bfloat16* mlp,
+                                                                        const float* site_feat,
+                                                                        int32_t* n_acc, int32_t* n_prop) {
+    const Dims& d = a.d;
+    const int i = blockIdx.x;
+    const GibbsPart gp = a.parts[i];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int K = gp.K;
+    double* spec = a.spec + (size_t)i * (a.Kcap + kAux) * kSpecStride;
+    double* ex = a.expt + (size_t)i * (a.Kcap + kAux) * d.N * d.R * kStates;
+    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * d.NI * 32;
+    const double* logits = a.logits + (size_t)i * (a.Kcap + kAux) * kStates;
+    int32_t* assign = a.assign + (size_t)i * d.S;
+    const double* base = a.base + (size_t)i * kBase;
+    extern __shared__ __align__(16) unsigned char lsm[];
+    __nv_bfloat16* W = reinterpret_cast<__nv_bfloat16*>(lsm);              // kMlpParams
+    float* xs = reinterpret_cast<float*>(lsm + ((kMlpParams * 2 + 15) & ~15));  // [warps][kMlpIn]
+    float* hs = xs + kGibbsWarps * kMlpIn;                                   // [warps][kMlpHid]
+    float* score = hs + kGibbsWarps * kMlpHid;                               // [Kcap]
+    int* counts = reinterpret_cast<int*>(score + a.Kcap);                   // [Kcap]
+    __shared__ double lrate[2][kMaxRates];
+    __shared__ float rev[2];
+    __shared__ int s_site, s_a, s_b;
+    __shared__ curandStatePhilox4_32_10_t rng_state;
+    __shared__ SpecWork work[kAux];
+    __shared__ int acc_n, prop_n;
+
+    for (int x = threadIdx.x; x < kMlpParams; x += blockDim.x) W[x] = mlp[x];
+    for (int k = threadIdx.x; k < a.Kcap; k += blockDim.x) counts[k] = 0;
+    if (threadIdx.x == 0) {
+        curand_init(a.seed, (unsigned long long)gp.p, 0ull, &rng_state);
+        acc_n = prop_n = 0;
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < d.S; x += blockDim.x) atomicAdd(&counts[assign[x]], 1);
+    if (warp < kAux)
+        for (int k = warp; k < K; k += kAux)
+            spectral_decompose_warp_ws(base, logits + (size_t)k * kStates, spec + (size_t)k * kSpecStride,
+                                       work[warp]);
+    __syncthreads();
+    for (int k = 0; k < K; ++k)
+        fill_exp(a, i, k, spec + (size_t)k * kSpecStride, ex + (size_t)k * d.N * d.R * kStates);
+    __syncthreads();
+    for (int it = 0; it < gp.n_iter; ++it) {
+        if (threadIdx.x == 0) {
+            int s = -1;
+            for (int tries = 0; tries < 64 && s < 0; ++tries) {
+                int c = (int)((1.0 - curand_uniform_double(&rng_state)) * d.S);
+                c = c < d.S ? c : d.S - 1;
+                if (counts[assign[c]] >= 2) s = c;  // the move never empties a class
+            }
+            s_site = s;
+        }
+        __syncthreads();
+        const int s = s_site;
+        if (s < 0) continue;
+        const float* sf = site_feat + (size_t)s * kSiteFeat;
+        for (int k = warp; k < K; k += kGibbsWarps) {  // forward scores
+            mlp_features(sf, spec + (size_t)k * kSpecStride + kSpecPi, counts[k], xs + warp * kMlpIn);
+            const float v = mlp_score(W, xs + warp * kMlpIn, hs + warp * kMlpHid);
+            if (lane == 0) score[k] = v;
+            __syncwarp();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float mx = -INFINITY;
+            for (int k = 0; k < K; ++k) mx = fmaxf(mx, score[k]);
+            double tot = 0.0;
+            for (int k = 0; k < K; ++k) tot += exp((double)(score[k] - mx));
+            const double draw = tot * curand_uniform_double(&rng_state);
+            double run = 0.0;
+            int b = K - 1;
+            for (int k = 0; k < K; ++k) {
+                run += exp((double)(score[k] - mx));
+                if (run >= draw) { b = k; break; }
+            }
+            s_a = assign[s];
+            s_b = b;
+            prop_n++;
+        }
+        __syncthreads();
+        const int ca = s_a, cb = s_b;
+        if (ca == cb) {  // proposing the current class: a no-op, always accepted
+            if (threadIdx.x == 0) acc_n++;
+            __syncthreads();
+            continue;
+        }
+        // Site likelihoods under the two classes (warps 0..R-1: a, R..2R-1: b),
+        // reverse scores with the updated class sizes (warps 2R, 2R+1).
+        if (warp < 2 * d.R) {
+            const int k = warp < d.R ? ca : cb, r = warp % d.R;
+            const double l = site_rate_lnl(a, i, s, r, spec + (size_t)k * kSpecStride,
+                                           ex + (size_t)k * d.N * d.R * kStates, stash);
+            if (lane == 0) lrate[warp < d.R ? 0 : 1][r] = l;
+        } else if (warp < 2 * d.R + 2) {
+            const int w = warp - 2 * d.R;
+            const int k = w == 0 ? ca : cb;
+            mlp_features(sf, spec + (size_t)k * kSpecStride + kSpecPi, counts[k] + (w == 0 ? -1 : 1),
+                         xs + warp * kMlpIn);
+            const float v = mlp_score(W, xs + warp * kMlpIn, hs + warp * kMlpHid);
+            if (lane == 0) rev[w] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const double la = site_value(a, gp, s, lrate[0], spec + (size_t)ca * kSpecStride + kSpecPi);
+            const double lb = site_value(a, gp, s, lrate[1], spec + (size_t)cb * kSpecStride + kSpecPi);
+            float mx = -INFINITY, mx2 = -INFINITY;
+            for (int k = 0; k < K; ++k) {
+                mx = fmaxf(mx, score[k]);
+                mx2 = fmaxf(mx2, k == ca ? rev[0] : (k == cb ? rev[1] : score[k]));
+            }
+            double z = 0.0, z2 = 0.0;
+            for (int k = 0; k < K; ++k) {
+                z += exp((double)(score[k] - mx));
+                z2 += exp((double)((k == ca ? rev[0] : (k == cb ? rev[1] : score[k])) - mx2));
+            }
+            const double lq_fwd = (score[cb] - mx) - log(z);
+            const double lq_rev = (rev[0] - mx2) - log(z2);
+            // CRP prior ratio n_b / (n_a - 1); tempered likelihood ratio.
+            const double lr = a.temp * (lb - la) + log((double)counts[cb]) - log((double)(counts[ca] - 1)) +
+                              lq_rev - lq_fwd;
+            if (log(curand_uniform_double(&rng_state)) <= lr) {
+                assign[s] = cb;
+                counts[ca]--;
+                counts[cb]++;
+                acc_n++;
+            }
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < K; k += blockDim.x) a.counts[(size_t)i * (a.Kcap + kAux) + k] = counts[k];
+    if (threadIdx.x == 0) {
+        a.kout[i] = K;
+        n_acc[i] = acc_n;
+        n_prop[i] = prop_n;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_learned_move(GibbsArgs a, const void* mlp, const float* site_feat, int32_t* n_acc,
+                                int32_t* n_prop, double* scratch, cudaStream_t st) {
+    const Dims& d = a.d;
+    if (2 * d.R + 2 > kGibbsWarps) return cudaErrorInvalidValue;
+    a.spec = scratch;
+    a.expt = a.spec + (size_t)a.count * (a.Kcap + kAux) * kSpecStride;
+    a.stash = a.expt + (size_t)a.count * (a.Kcap + kAux) * d.N * d.R * kStates;
+    const size_t smem = ((kMlpParams * 2 + 15) & ~15) +
+                        sizeof(float) * (kGibbsWarps * (kMlpIn + kMlpHid) + a.Kcap) + sizeof(int) * a.Kcap;
+    cudaError_t e = cudaFuncSetAttribute(learned_move_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    learned_move_kernel<<<a.count, 32 * kGibbsWarps, smem, st>>>(
+        a, static_cast<const __nv_bfloat16*>(mlp), site_feat, n_acc, n_prop);
+    return cudaGetLastError();
+}
 
 size_t gibbs_scratch_doubles(const Dims& d, int count, int Kcap) {
     const size_t spec = (size_t)count * (Kcap + kAux) * kSpecStride;

@@ -46,4 +46,10 @@ size_t gibbs_scratch_doubles(const Dims& d, int count, int Kcap);
 int gibbs_aux();
 cudaError_t launch_gibbs(GibbsArgs a, double* scratch, cudaStream_t st);
 
+// Learned-proposal MH site reassignment: parts[i].n_iter updates per particle
+// among its existing classes, proposals from the scoring MLP (BF16 weights
+// `mlp`, site features [S][21]); accepted / proposed counts per particle.
+cudaError_t launch_learned_move(GibbsArgs a, const void* mlp, const float* site_feat,
+                                int32_t* n_acc, int32_t* n_prop, double* scratch, cudaStream_t st);
+
 }  // namespace smccat

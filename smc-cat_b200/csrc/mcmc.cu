@@ -592,12 +592,20 @@ namespace {
 
 // Runs the device Gibbs kernel on the listed particles. In weights mode
 // (site >= 0) only writes the weight vector of particle list[0] and changes
-// nothing; otherwise installs the new class sets and refreshes.
+// nothing; otherwise installs the new class sets and refreshes. With
+// `learned_updates` > 0 the learned-proposal MH move runs instead of Gibbs.
 int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, uint64_t seed,
-              int site, const double* aux, double* weights_out, smccat_gibbs_stats* stats) {
+              int site, const double* aux, double* weights_out, smccat_gibbs_stats* stats,
+              int learned_updates = 0, smccat_learned_stats* lstats = nullptr) {
     const Dims& d = dims_of(c);
     const int n = (int)list.size();
     if (n == 0) return SMCCAT_OK;
+    const float* site_feat = nullptr;
+    const void* mlp = nullptr;
+    if (learned_updates > 0) {
+        mlp = learned_inference_weights(c, &site_feat);
+        if (!mlp) return mfail(SMCCAT_ESTATE, "the learned proposal has not been trained");
+    }
     const int naux = gibbs_aux();
     const int Kcap = d.Kmax + 64;
     const int ks = Kcap + naux;
@@ -611,7 +619,7 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         GibbsPart& g = parts[j];
         g.p = list[j];
         g.K = m.K;
-        g.n_iter = site >= 0 ? 1 : d.S / 2;  // Particle.cpp:791
+        g.n_iter = learned_updates > 0 ? learned_updates : (site >= 0 ? 1 : d.S / 2);  // Particle.cpp:791
         g.fixed_site = site;
         g.pinv = m.pinv;
         for (int r = 0; r < kMaxRates; ++r) g.rates[r] = m.rates[r];
@@ -641,7 +649,8 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
                  o_logits = carve(logits.size() * 8), o_assign = carve(assign.size() * 4),
                  o_counts = carve((size_t)n * ks * 4), o_kout = carve((size_t)n * 4),
                  o_aux = carve(auxv.size() * 8), o_w = carve((size_t)n * ks * 8),
-                 o_status = carve(4), o_scr = carve(scratch * 8);
+                 o_status = carve(4), o_scr = carve(scratch * 8), o_acc = carve((size_t)n * 4),
+                 o_prop = carve((size_t)n * 4);
     char* dbuf = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&dbuf, bytes, st);
     if (e != cudaSuccess) return mfail(SMCCAT_ENOMEM, std::string("gibbs buffers: ") + cudaGetErrorString(e));
@@ -684,7 +693,12 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         a.isinv = isinv_device(c);
         a.invchar = invchar_device(c);
         a.status = reinterpret_cast<int*>(dbuf + o_status);
-        e = launch_gibbs(a, reinterpret_cast<double*>(dbuf + o_scr), st);
+        if (learned_updates > 0)
+            e = launch_learned_move(a, mlp, site_feat, reinterpret_cast<int32_t*>(dbuf + o_acc),
+                                    reinterpret_cast<int32_t*>(dbuf + o_prop),
+                                    reinterpret_cast<double*>(dbuf + o_scr), st);
+        else
+            e = launch_gibbs(a, reinterpret_cast<double*>(dbuf + o_scr), st);
     }
     down(assign.data(), o_assign, assign.size() * 4);
     down(counts.data(), o_counts, counts.size() * 4);
@@ -692,9 +706,18 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     down(logits.data(), o_logits, logits.size() * 8);
     down(wout.data(), o_w, wout.size() * 8);
     down(&status, o_status, 4);
+    std::vector<int32_t> nacc(n, 0), nprop(n, 0);
+    if (learned_updates > 0) {
+        down(nacc.data(), o_acc, (size_t)n * 4);
+        down(nprop.data(), o_prop, (size_t)n * 4);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFreeAsync(dbuf, st);
     if (e != cudaSuccess) return mfail(SMCCAT_ECUDA, std::string("gibbs: ") + cudaGetErrorString(e));
+    if (lstats) {
+        *lstats = smccat_learned_stats{};
+        for (int j = 0; j < n; ++j) { lstats->proposed += nprop[j]; lstats->accepted += nacc[j]; }
+    }
     if (site >= 0) {
         const int K = slot_of(c, list[0]).cur.K;
         for (int k = 0; k < K; ++k) weights_out[k] = wout[k];
@@ -759,6 +782,23 @@ int smccat_gibbs(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* mas
         list.push_back(first + i);
     }
     return run_gibbs(c, list, temperature, seed, -1, nullptr, nullptr, stats);
+}
+
+int smccat_learned_move(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* mask,
+                        int32_t updates, double temperature, uint64_t seed,
+                        smccat_learned_stats* stats) {
+    if (!c || first < 0 || count < 0 || updates < 1) return mfail(SMCCAT_EINVAL, "bad argument");
+    if (!(model_flags_of(c) & SMCCAT_MODEL_CAT)) return mfail(SMCCAT_EINVAL, "the learned move needs SMCCAT_MODEL_CAT");
+    if (2 * dims_of(c).R + 2 > 16) return mfail(SMCCAT_EINVAL, "the learned move supports at most 7 rates");
+    std::vector<int> list;
+    for (int i = 0; i < count; ++i) {
+        if (mask && !mask[i]) continue;
+        const Slot& s = slot_of(c, first + i);
+        if (!s.loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
+        if (s.pending) return mfail(SMCCAT_ESTATE, "particle has uncommitted edits");
+        list.push_back(first + i);
+    }
+    return run_gibbs(c, list, temperature, seed, -1, nullptr, nullptr, nullptr, updates, stats);
 }
 
 int smccat_gibbs_weights(smccat_ctx* c, int32_t p, int32_t site, const double* aux_logits,

@@ -64,6 +64,14 @@ class GibbsStats(ctypes.Structure):
                 ("classes_after", ctypes.c_int64), ("created", ctypes.c_int64)]
 
 
+class LearnedStats(ctypes.Structure):
+    _fields_ = [("proposed", ctypes.c_int64), ("accepted", ctypes.c_int64)]
+
+
+MLP_PARAMS, MLP_INPUTS = 22401, 44
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
 class Config(ctypes.Structure):
     _fields_ = [("num_taxa", _i32), ("num_sites", _i32), ("num_rates", _i32),
                 ("max_particles", _i32), ("max_classes", _i32), ("model_flags", _i32),
@@ -129,6 +137,12 @@ def lib():
         "smccat_gibbs": ([vp, _i32, _i32, _up, ctypes.c_double, ctypes.c_uint64,
                           ctypes.POINTER(GibbsStats)], ctypes.c_int),
         "smccat_gibbs_weights": ([vp, _i32, _i32, _dp, ctypes.c_double, _dp], ctypes.c_int),
+        "smccat_learned_train": ([vp, _i32, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64,
+                                  _dp], ctypes.c_int),
+        "smccat_learned_gradients": ([vp, _i32, _ip, _fp, _ip, _fp, _dp], ctypes.c_int),
+        "smccat_learned_params": ([vp, _fp, _fp], ctypes.c_int),
+        "smccat_learned_move": ([vp, _i32, _i32, _up, _i32, ctypes.c_double, ctypes.c_uint64,
+                                 ctypes.POINTER(LearnedStats)], ctypes.c_int),
         "smccat_get_profile": ([vp, ctypes.POINTER(Profile)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -364,6 +378,44 @@ class Engine:
         _check(lib().smccat_gibbs_weights(self._h, int(p), int(site), ap, float(temperature),
                                           out.ctypes.data_as(_dp)))
         return out
+
+    # -- learned CAT proposal ------------------------------------------------
+    def learned_train(self, epochs, batch_sites=512, lr=1e-3, seed=0, first=0, count=None):
+        count = self.P - first if count is None else count
+        loss = ctypes.c_double(0.0)
+        _check(lib().smccat_learned_train(self._h, int(first), int(count), int(epochs),
+                                          int(batch_sites), float(lr), int(seed), ctypes.byref(loss)))
+        return loss.value
+
+    def learned_params(self, set_to=None) -> np.ndarray:
+        out = np.zeros(MLP_PARAMS, dtype=np.float32)
+        src = None
+        if set_to is not None:
+            src = np.ascontiguousarray(set_to, dtype=np.float32)
+        _check(lib().smccat_learned_params(self._h, out.ctypes.data_as(_fp),
+                                           src.ctypes.data_as(_fp) if src is not None else None))
+        return out
+
+    def learned_gradients(self, x, group_off, labels):
+        xx = np.ascontiguousarray(x, dtype=np.float32)
+        off, offp = _i(group_off)
+        lab, labp = _i(labels)
+        g = np.zeros(MLP_PARAMS, dtype=np.float32)
+        loss = ctypes.c_double(0.0)
+        _check(lib().smccat_learned_gradients(self._h, len(lab), offp, xx.ctypes.data_as(_fp), labp,
+                                              g.ctypes.data_as(_fp), ctypes.byref(loss)))
+        return loss.value, g
+
+    def learned_move(self, updates, temperature, seed, mask=None, first=0, count=None) -> dict:
+        count = self.P - first if count is None else count
+        st = LearnedStats()
+        mp = None
+        if mask is not None:
+            m = np.ascontiguousarray(mask, dtype=np.uint8)
+            mp = m.ctypes.data_as(_up)
+        _check(lib().smccat_learned_move(self._h, int(first), int(count), mp, int(updates),
+                                         float(temperature), int(seed), ctypes.byref(st)))
+        return {"proposed": int(st.proposed), "accepted": int(st.accepted)}
 
     def smc_step(self, raw_weights, target_ess, last_temp, first=0):
         w = np.array(raw_weights, dtype=np.float64, copy=True)

@@ -1,0 +1,80 @@
+"""The learned CAT class proposal: device gradients against the CPU oracle, and
+what the trained network gains over an untrained (uniform) proposal."""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import mlp as omlp
+import smccat
+from smccat import workload
+
+pytestmark = pytest.mark.gpu
+
+
+def cat_engine(seed=31, n=8, S=240):
+    cfg = workload.WorkloadConfig("learned", T=10, S=S, R=4, particles=n, iterations=2,
+                                  lg=False, invar=False, cat=True, alpha=0.8,
+                                  dp_concentration=3.0, k_range=(4, 6), seed=seed)
+    rng = np.random.default_rng(seed)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    st = workload.make_particles(cfg, n, rng, kmax=16)
+    eng = smccat.Engine(codes, cfg.R, n, max_classes=16, cat=True)
+    eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                      st["logits"], st["assign"], st["pinv"], st["shape"])
+    eng.refresh(full=True)
+    return eng, codes, cfg
+
+
+def test_gradients_match_cpu_oracle():
+    eng, codes, cfg = cat_engine(n=2)
+    rng = np.random.default_rng(4)
+    params = (rng.normal(size=omlp.N_PARAMS) * 0.1).astype(np.float32)
+    eng.learned_params(set_to=params)
+    sizes = [3, 5, 2, 6, 4, 1, 7]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    X = rng.normal(size=(off[-1], omlp.IN)).astype(np.float32)
+    labels = np.array([rng.integers(s) for s in sizes], dtype=np.int32)
+    loss, g = eng.learned_gradients(X, off, labels)
+    rloss, rg = omlp.loss_and_grad(params.astype(np.float64), X.astype(np.float64), off, labels)
+    assert loss == pytest.approx(rloss, rel=1e-4)
+    scale = np.abs(rg).max()
+    np.testing.assert_allclose(g, rg, atol=2e-4 * scale, rtol=1e-3)
+    # finite-difference check of the oracle itself on a few coordinates
+    for idx in (0, omlp.IN * omlp.HID + 3, omlp.N_PARAMS - 1):
+        e = np.zeros(omlp.N_PARAMS)
+        e[idx] = 1e-6
+        p64 = params.astype(np.float64)
+        fd = (omlp.loss_and_grad(p64 + e, X, off, labels)[0]
+              - omlp.loss_and_grad(p64 - e, X, off, labels)[0]) / 2e-6
+        assert fd == pytest.approx(rg[idx], rel=1e-4, abs=1e-7)
+    eng.close()
+
+
+def test_trained_proposal_beats_uniform_and_keeps_exact_likelihoods():
+    eng, codes, cfg = cat_engine()
+    # Gibbs warm-up produces the training assignments.
+    for call in range(4):
+        eng.gibbs(temperature=1.0, seed=10 + call)
+    # Untrained network (all-zero weights): a uniform proposal over classes.
+    eng.learned_params(set_to=np.zeros(smccat.MLP_PARAMS, np.float32))
+    base = eng.learned_move(updates=400, temperature=1.0, seed=5)
+    # Train from a fresh initialisation (Glorot) on the Gibbs samples.
+    eng.learned_params(set_to=(np.random.default_rng(1).normal(size=smccat.MLP_PARAMS) * 0.05)
+                       .astype(np.float32))
+    loss = eng.learned_train(epochs=30, batch_sites=256, lr=3e-3, seed=2)
+    k_mean = eng.get_particles()["num_classes"].mean()
+    assert loss < 0.9 * np.log(k_mean), (loss, np.log(k_mean))   # better than chance
+    trained = eng.learned_move(updates=400, temperature=1.0, seed=5)
+    acc_base = base["accepted"] / base["proposed"]
+    acc_trained = trained["accepted"] / trained["proposed"]
+    assert acc_trained > acc_base, (acc_trained, acc_base)
+    fin = eng.get_particles()
+    got = eng.lnl()
+    for i in range(cfg.particles):
+        K = int(fin["num_classes"][i])
+        assert np.all(np.bincount(fin["assign"][i], minlength=K) > 0)
+        rates = oracle.discretize_gamma(fin["shape"][i], cfg.R)
+        ref = oracle.lnl(codes, fin["parent"][i], fin["branch"][i], fin["base"][i],
+                         fin["logits"][i][:K], fin["assign"][i], fin["pinv"][i], rates)
+        assert got[i] == pytest.approx(ref, rel=1e-9)
+    eng.close()
