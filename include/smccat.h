@@ -389,6 +389,12 @@ typedef struct smccat_profile {
  * particles must have no pending edits; their likelihoods are recomputed. */
 int smccat_autotune(smccat_ctx* ctx, int32_t reps, int32_t* variant_out, double* ms_out);
 
+/* Number of pruning-kernel variants of this context (FP64 contexts: SIMT
+ * kernels at three register caps, then FP64 tensor-path kernels), the one in
+ * use, and a way to pin one (what smccat_autotune sets). */
+int smccat_kernel_variants(smccat_ctx* ctx, int32_t* count, int32_t* current);
+int smccat_set_kernel_variant(smccat_ctx* ctx, int32_t variant);
+
 /* Enable (1) or disable (0) per-launch CUDA-event timing; resets counters. */
 int smccat_set_profiling(smccat_ctx* ctx, int32_t enable);
 

@@ -890,7 +890,7 @@ int smccat_autotune(smccat_ctx* c, int32_t reps, int32_t* variant_out, double* m
     reps = std::max(1, reps);
     const bool timing = c->timing;
     const smccat_profile saved = c->prof;
-    const int nv = prune_variants(c->d.R);
+    const int nv = prune_variants(c->d.R, c->esz == 4);
     int best = 0;
     double best_ms = INFINITY;
     for (int v = 0; v < nv; ++v) {
@@ -917,6 +917,21 @@ int smccat_autotune(smccat_ctx* c, int32_t reps, int32_t* variant_out, double* m
     c->ev_used.clear();
     c->prof = saved;
     if (variant_out) *variant_out = best;
+    return SMCCAT_OK;
+}
+
+int smccat_kernel_variants(smccat_ctx* c, int32_t* count, int32_t* current) {
+    if (!c) return fail(SMCCAT_EINVAL, "null context");
+    if (count) *count = prune_variants(c->d.R, c->esz == 4);
+    if (current) *current = c->prune_variant;
+    return SMCCAT_OK;
+}
+
+int smccat_set_kernel_variant(smccat_ctx* c, int32_t variant) {
+    if (!c) return fail(SMCCAT_EINVAL, "null context");
+    if (variant < 0 || variant >= prune_variants(c->d.R, c->esz == 4))
+        return fail(SMCCAT_EINVAL, "kernel variant out of range");
+    c->prune_variant = variant;
     return SMCCAT_OK;
 }
 

@@ -36,9 +36,12 @@ struct PruneArgs {
 cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d, cudaStream_t st);
 cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, const uint8_t* sws,
                         const double* spec, void* Pm, bool fp32, const Dims& d, cudaStream_t st);
-// Pruning kernel variants (register caps) available for R rate categories.
-int prune_variants(int R);
+// Pruning kernel variants available for R rate categories: SIMT kernels at
+// several register caps, then (FP64 only) the FP64 tensor-path kernels.
+int prune_variants(int R, bool fp32);
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
+int prune_dmma_variants(int R);
+cudaError_t launch_prune_dmma(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
 cudaError_t launch_reduce(const int32_t* tile_off, const double* partial, const PartHdr* hdr, int first,
                           int count, double* lnl, int* status, cudaStream_t st);
 cudaError_t launch_accept(double* lnl, double* lnl_old, const uint8_t* mask, int first, int count,

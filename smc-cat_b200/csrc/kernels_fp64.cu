@@ -470,12 +470,22 @@ cudaError_t launch_prune_typed(const PruneArgs& a, int ntiles, int variant, cuda
 
 }  // namespace
 
-int prune_variants(int R) { return R == 4 ? 3 : 1; }
+namespace {
+int simt_variants(int R) { return R == 4 ? 3 : 1; }
+}  // namespace
+
+// FP64 contexts also have the tensor-path (DMMA) kernels, numbered after the
+// SIMT ones.
+int prune_variants(int R, bool fp32) {
+    return simt_variants(R) + (fp32 ? 0 : prune_dmma_variants(R));
+}
 
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
     if (ntiles <= 0) return cudaSuccess;
-    return a.fp32 ? launch_prune_typed<float>(a, ntiles, variant, st)
-                  : launch_prune_typed<double>(a, ntiles, variant, st);
+    if (a.fp32) return launch_prune_typed<float>(a, ntiles, variant, st);
+    const int ns = simt_variants(a.d.R);
+    if (variant >= ns) return launch_prune_dmma(a, ntiles, variant - ns, st);
+    return launch_prune_typed<double>(a, ntiles, variant, st);
 }
 
 cudaError_t launch_reduce(const int32_t* tile_off, const double* partial, const PartHdr* hdr, int first,

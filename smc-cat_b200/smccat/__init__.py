@@ -123,6 +123,8 @@ def lib():
         "smccat_get_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
         "smccat_set_profiling": ([vp, _i32], ctypes.c_int),
         "smccat_autotune": ([vp, _i32, _ip, _dp], ctypes.c_int),
+        "smccat_kernel_variants": ([vp, _ip, _ip], ctypes.c_int),
+        "smccat_set_kernel_variant": ([vp, _i32], ctypes.c_int),
         "smccat_set_tuning": ([vp, ctypes.POINTER(Tuning)], ctypes.c_int),
         "smccat_get_tuning": ([vp, ctypes.POINTER(Tuning)], ctypes.c_int),
         "smccat_set_rate_cholesky": ([vp, _dp], ctypes.c_int),
@@ -441,6 +443,15 @@ class Engine:
         ms = np.full(8, np.nan)
         _check(lib().smccat_autotune(self._h, int(reps), ctypes.byref(v), ms.ctypes.data_as(_dp)))
         return {"variant": int(v.value), "ms": [float(x) for x in ms if not np.isnan(x)]}
+
+    def kernel_variants(self):
+        """(number of pruning-kernel variants, the one in use)."""
+        n, cur = ctypes.c_int32(0), ctypes.c_int32(0)
+        _check(lib().smccat_kernel_variants(self._h, ctypes.byref(n), ctypes.byref(cur)))
+        return int(n.value), int(cur.value)
+
+    def set_kernel_variant(self, v: int):
+        _check(lib().smccat_set_kernel_variant(self._h, int(v)))
 
     def set_profiling(self, enable: bool):
         _check(lib().smccat_set_profiling(self._h, 1 if enable else 0))
