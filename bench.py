@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--sweep-temp", type=float, default=0.5)
     ap.add_argument("--mixed", type=int, default=1,
                     help="also time the FP32 (mixed-precision) path on the same particles")
+    ap.add_argument("--extra-configs", default="",
+                    help="comma-separated CAT configs (e.g. 3,4) to time in particle waves")
+    ap.add_argument("--extra-particles", type=int, default=0,
+                    help="particles for --extra-configs (default: the configuration's)")
     return ap.parse_args()
 
 
@@ -189,6 +193,76 @@ def cpu_baseline(cfg, codes, st, n_sample, min_seconds=10.0):
     return {"value": units / el, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{n} particles x {cfg.S} sites x {cfg.R} categories, full refresh, "
                       f"{reps} repetitions in {el:.1f} s (FP64 oracle, OpenMP over particles)"}
+
+
+def measure_config_waves(cid, steps, local, rank, particles=0, oracle_sample=2):
+    """Full-refresh throughput of a configuration whose particles may not fit
+    one context: particles stream through the device in waves (upload states,
+    refreshLikelihood(true), read log-likelihoods), at FP64 and at FP32; the
+    FP32 log-likelihoods are compared with FP64 per particle, and a few
+    particles of both with the oracle."""
+    import torch
+    import oracle
+    import smccat
+    from smccat import discretize_gamma, workload
+    cfg = workload.CONFIGS[cid]
+    rng = np.random.default_rng(cfg.seed)
+    codes, truth = workload.simulate_alignment(cfg, rng)
+    n = particles or cfg.particles
+    st = workload.make_particles(cfg, n, np.random.default_rng(cfg.seed * 1000 + rank))
+    kmax = st["logits"].shape[1]
+    res = {"workload": cfg.name, "taxa": cfg.T, "sites": cfg.S, "rates": cfg.R, "particles": n,
+           "max_classes": kmax, "data_classes": int(truth["K"])}
+    lnls = {}
+    for prec, name in ((smccat.PREC_FP64, "fp64"), (smccat.PREC_FP32, "fp32")):
+        esz = 4 if prec == smccat.PREC_FP32 else 8
+        spad = (cfg.S + 31) // 32 * 32
+        per = (cfg.T - 1) * 2 * (20 * esz + 8) * cfg.R * spad + \
+            kmax * (2 * cfg.T - 1) * 2 * cfg.R * 440 * esz + 4 * cfg.S + 8 * cfg.S
+        free = torch.cuda.mem_get_info(local)[0]
+        W = max(1, min(n, int(0.8 * free / per)))
+        eng = smccat.Engine(codes, cfg.R, W, max_classes=kmax, lg=cfg.lg, invar=cfg.invar,
+                            cat=cfg.cat, device=local, precision=prec)
+        stream = torch.cuda.ExternalStream(eng.stream_ptr, device=torch.device("cuda", local))
+
+        def one_pass():
+            out = []
+            for w0 in range(0, n, W):
+                c = min(W, n - w0)
+                sl = slice(w0, w0 + c)
+                eng.set_particles(0, st["parent"][sl], st["branch"][sl], st["base"][sl],
+                                  st["num_classes"][sl], st["logits"][sl], st["assign"][sl],
+                                  st["pinv"][sl], st["shape"][sl])
+                eng.refresh(0, c, full=True)
+                out.append(eng.lnl(0, c))
+            return np.concatenate(out)
+
+        lnls[name] = one_pass()
+        eng.autotune(reps=1) if n <= W else None
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            one_pass()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res[name] = {"value": n * cfg.S * cfg.R / (ms * 1e-3), "unit": UNIT, "ms_per_pass": ms,
+                     "particles_per_wave": W, "waves": (n + W - 1) // W,
+                     "device_gb": eng.device_bytes / 1e9}
+        eng.close()
+    d = np.abs(lnls["fp32"] - lnls["fp64"])
+    res["fp32_vs_fp64_abs_dlogl"] = {"max": float(d.max()), "mean": float(d.mean())}
+    o = []
+    for i in range(min(oracle_sample, n)):
+        K = int(st["num_classes"][i])
+        rates = discretize_gamma(st["shape"][i], cfg.R)
+        ref = oracle.lnl(codes, st["parent"][i], st["branch"][i], st["base"][i],
+                         st["logits"][i][:K], st["assign"][i], st["pinv"][i], rates)
+        o.append({"fp64_rel": abs(lnls["fp64"][i] - ref) / abs(ref),
+                  "fp32_abs": abs(lnls["fp32"][i] - ref)})
+    res["vs_oracle"] = o
+    return res
 
 
 def run_reference(args, rank, world):
@@ -439,6 +513,11 @@ def main():
                 "accepted": sum(sweep_stats["accepted"])},
             "clocks": clk,
         }
+        if args.extra_configs:
+            line["extra_configs"] = [
+                measure_config_waves(int(c), max(1, args.steps // 5), local, rank,
+                                     particles=args.extra_particles)
+                for c in args.extra_configs.split(",") if c.strip()]
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(cfg, codes, st, args.cpu_sample)
         print(json.dumps(line), flush=True)
