@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=32,
                     help="particles per CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="pin this pruning-kernel variant instead of autotuning (profiling)")
     ap.add_argument("--particles", type=int, default=0,
                     help="override the particle count (small cases for ncu captures)")
     ap.add_argument("--skip-e2e", action="store_true")
@@ -342,7 +344,11 @@ def main():
                                      st["shape"])
     load()
     eng.refresh(full=True)
-    tuned = eng.autotune(reps=2)
+    if args.variant >= 0:
+        eng.set_kernel_variant(args.variant)
+        tuned = {"variant": args.variant, "ms": None}
+    else:
+        tuned = eng.autotune(reps=2)
     stream = torch.cuda.ExternalStream(eng.stream_ptr, device=torch.device("cuda", local))
     units_per_step = n * cfg.S * cfg.R
 

@@ -80,6 +80,7 @@ struct smccat_ctx {
     size_t plan_cap = 0;
     int tile_cap = 0;
     int prune_variant = 0;      // chosen by smccat_autotune
+    int tile_sites = kTileSites;  // slots per pruning tile, as the variant expects
 
     std::vector<uint8_t> codes;
     std::vector<Slot> slots;
@@ -213,9 +214,9 @@ cudaError_t launch(smccat_ctx* c, int kind, F&& f) {
     return e;
 }
 
-// Sites grouped by class (stable), then cut into tiles of <= kTileSites.
+// Sites grouped by class (stable), then cut into tiles of <= tile_sites.
 void rebuild_tiles(smccat_ctx* c) {
-    const int P = c->cfg.max_particles, S = c->d.S;
+    const int P = c->cfg.max_particles, S = c->d.S, ts = c->tile_sites;
     c->tiles.clear();
     c->tile_off.assign(P + 1, 0);
     for (int p = 0; p < P; ++p) {
@@ -226,12 +227,23 @@ void rebuild_tiles(smccat_ctx* c) {
         for (int i = 0; i < S; ++i) cnt[s.assign[i]]++;
         int slot0 = 0;
         for (int k = 0; k < s.cur.K; ++k) {
-            for (int off = 0; off < cnt[k]; off += kTileSites)
-                c->tiles.push_back(Tile{p, k, slot0 + off, std::min(kTileSites, cnt[k] - off)});
+            for (int off = 0; off < cnt[k]; off += ts)
+                c->tiles.push_back(Tile{p, k, slot0 + off, std::min(ts, cnt[k] - off)});
             slot0 += cnt[k];
         }
     }
     c->tile_off[P] = (int)c->tiles.size();
+}
+
+// Select pruning variant v; a different tile width rebuilds the tile list at
+// the next refresh.
+void select_variant(smccat_ctx* c, int v) {
+    c->prune_variant = v;
+    const int ts = prune_variant_tile_sites(c->d.R, c->esz == 4, v);
+    if (ts != c->tile_sites) {
+        c->tile_sites = ts;
+        c->tiles_dirty = true;
+    }
 }
 
 }  // namespace
@@ -894,7 +906,7 @@ int smccat_autotune(smccat_ctx* c, int32_t reps, int32_t* variant_out, double* m
     int best = 0;
     double best_ms = INFINITY;
     for (int v = 0; v < nv; ++v) {
-        c->prune_variant = v;
+        select_variant(c, v);
         int rc = smccat_refresh(c, 0, n, SMCCAT_REFRESH_FULL);  // warm-up, also commits loads
         if (rc) return rc;
         c->timing = true;
@@ -912,7 +924,7 @@ int smccat_autotune(smccat_ctx* c, int32_t reps, int32_t* variant_out, double* m
         if (ms < best_ms) { best_ms = ms; best = v; }
         c->timing = false;
     }
-    c->prune_variant = best;
+    select_variant(c, best);
     c->timing = timing;
     c->ev_used.clear();
     c->prof = saved;
@@ -931,7 +943,7 @@ int smccat_set_kernel_variant(smccat_ctx* c, int32_t variant) {
     if (!c) return fail(SMCCAT_EINVAL, "null context");
     if (variant < 0 || variant >= prune_variants(c->d.R, c->esz == 4))
         return fail(SMCCAT_EINVAL, "kernel variant out of range");
-    c->prune_variant = variant;
+    select_variant(c, variant);
     return SMCCAT_OK;
 }
 

@@ -39,6 +39,8 @@ cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, 
 // Pruning kernel variants available for R rate categories: SIMT kernels at
 // several register caps, then (FP64 only) the FP64 tensor-path kernels.
 int prune_variants(int R, bool fp32);
+// Slots per pruning tile that a variant expects (32 or 64).
+int prune_variant_tile_sites(int R, bool fp32, int variant);
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
 int prune_dmma_variants(int R);
 cudaError_t launch_prune_dmma(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);

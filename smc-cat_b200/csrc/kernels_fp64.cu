@@ -5,10 +5,10 @@
 //   pmat_kernel   one CTA per (particle, node): P(t r) = L diag(exp(lambda t r)) Rm
 //                 for every class and rate (TransitionProbabilityClass.cpp:83-95),
 //                 row-major with a row-sum column.
-//   prune_kernel  one warp per (rate, tile of <= 32 same-class sites), R warps per
-//                 CTA: walks the particle's dirty internal nodes in post-order
-//                 (Particle.cpp:577-626). Each warp stages its two children's P
-//                 blocks into shared memory with TMA bulk copies (double-buffered,
+//   prune_kernel  one warp per (rate, tile of <= 32 W same-class sites, W sites
+//                 per lane), R warps per CTA: walks the particle's dirty
+//                 internal nodes in post-order (Particle.cpp:577-626). Each warp
+//                 stages its two children's P blocks into shared memory with TMA bulk copies (double-buffered,
 //                 mbarrier-tracked, the next node's copy in flight while the
 //                 current node computes), keeps the partial it just produced in
 //                 registers (in a post-order of an upward-closed dirty set the
@@ -90,21 +90,44 @@ __device__ __forceinline__ int exponent_of(float mx) { int e; frexpf(mx, &e); re
 __device__ __forceinline__ double pow2(double, int e) { return ldexp(1.0, e); }
 __device__ __forceinline__ float pow2(float, int e) { return ldexpf(1.0f, e); }
 
-// acc[i] = sum_j P[i][j] x[j] with P row-major (stride kPCols), broadcast reads.
-template <class T>
-__device__ __forceinline__ void matvec(const T* __restrict__ P, const T* x, T* acc) {
+// acc[w][i] = sum_j P[i][j] x[w][j] for the W sites of a lane, P row-major
+// (stride kPCols) in shared memory, every lane reading the same element.
+// MUL: multiply the result into acc instead of assigning it.
+// Row dot products, RB rows in flight (2 RB independent FMA chains), P read
+// as pairs: each shared-memory load feeds 2 W FMAs.
+template <class T, int W, bool MUL, int RB>
+__device__ __forceinline__ void matvec(const T* __restrict__ P, const T (*x)[kStates],
+                                       T (*acc)[kStates]) {
+    static_assert(kStates % RB == 0, "rows in flight must divide the state count");
     using P2 = typename Pair<T>::type;
 #pragma unroll
-    for (int i = 0; i < kStates; ++i) {
-        const P2* row = reinterpret_cast<const P2*>(P + i * kPCols);
-        T s0 = 0, s1 = 0;
+    for (int i0 = 0; i0 < kStates; i0 += RB) {
+        T s0[RB][W], s1[RB][W];
+#pragma unroll
+        for (int b = 0; b < RB; ++b) {
+#pragma unroll
+            for (int w = 0; w < W; ++w) s0[b][w] = s1[b][w] = 0;
+        }
 #pragma unroll
         for (int j = 0; j < kStates / 2; ++j) {
-            const P2 p2 = row[j];
-            s0 = fma(p2.x, x[2 * j], s0);
-            s1 = fma(p2.y, x[2 * j + 1], s1);
+#pragma unroll
+            for (int b = 0; b < RB; ++b) {
+                const P2 p2 = reinterpret_cast<const P2*>(P + (i0 + b) * kPCols)[j];
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    s0[b][w] = fma(p2.x, x[w][2 * j], s0[b][w]);
+                    s1[b][w] = fma(p2.y, x[w][2 * j + 1], s1[b][w]);
+                }
+            }
         }
-        acc[i] = s0 + s1;
+#pragma unroll
+        for (int b = 0; b < RB; ++b) {
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                if (MUL) acc[w][i0 + b] *= s0[b][w] + s1[b][w];
+                else acc[w][i0 + b] = s0[b][w] + s1[b][w];
+            }
+        }
     }
 }
 
@@ -176,10 +199,13 @@ __global__ void __launch_bounds__(128) pmat_kernel(const PJob* __restrict__ jobs
 // Pruning + root reduction of one tile: warp r handles rate category r.
 // MINB = CTAs per SM the register allocation must allow (the register cap is
 // 65536 / (32 R MINB)); the autotuner picks among the instantiated values.
+// W = sites per lane: the tile has up to 32 W slots, lane l owning slots
+// l, l + 32, ...; W = 2 halves the shared-memory loads per FMA at the cost of
+// registers. RB = mat-vec rows in flight (see matvec).
 // T = storage and arithmetic type of partials and transition matrices
 // (double, or float for the mixed-precision path); log-scalers and the root
 // reduction are FP64 in both.
-template <class T, int R, int MINB>
+template <class T, int R, int MINB, int W, int RB>
 __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) {
     const Dims d = a.d;
     const int tile_id = a.tile_begin + blockIdx.x;
@@ -187,18 +213,26 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     const int p = tl.p;
     const PartHdr* h = a.hdr + (p - a.first);
     if (!h->active) return;  // uniform across the CTA
-    using P2 = typename Pair<T>::type;
     constexpr uint32_t kPBytes = kPBlock * sizeof(T);
 
     extern __shared__ __align__(128) unsigned char smem_raw[];  // [R warps][2 buffers][2 children][kPBlock]
     __shared__ __align__(8) uint64_t bars[R][2];
-    __shared__ double red[R][32];
+    __shared__ double red[R][32 * W];
     __shared__ int bad;
 
     const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
-    const bool valid = lane < tl.nslots;
-    const int slot = tl.slot0 + (valid ? lane : 0);
-    const int site = a.perm[(size_t)p * d.S + slot];
+    const bool valid = lane < tl.nslots;  // the lane owns at least one slot
+    // A lane's unused slots alias its first slot (or the tile's first): they
+    // are computed like the others and never stored.
+    bool vw[W];
+    int site[W], col[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        vw[w] = lane + 32 * w < tl.nslots;
+        const int slot = tl.slot0 + (vw[w] ? lane + 32 * w : (valid ? lane : 0));
+        site[w] = a.perm[(size_t)p * d.S + slot];
+        col[w] = r * d.Spad + slot;
+    }
     T* buf = reinterpret_cast<T*>(smem_raw) + (size_t)r * 4 * kPBlock;
 
     const size_t j_stride = (size_t)R * d.Spad;
@@ -207,7 +241,6 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     const size_t lws_stride = j_stride;
     T* CLp = static_cast<T*>(a.CL) + (size_t)p * d.NI * node_stride;
     double* LSCp = a.LSC + (size_t)p * d.NI * 2 * lws_stride;
-    const int col = r * d.Spad + slot;
     const T* Pcls = static_cast<const T*>(a.Pm) +
                     ((size_t)p * d.Kmax + tl.k) * d.N * 2 * (size_t)R * kPBlock + (size_t)r * kPBlock;
     auto pblock = [&](int child, int pws) {
@@ -231,8 +264,10 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
         tma_load_1d(buf + kPBlock, pblock(nj.c2, (nj.ws >> 4) & 1), kPBytes, &bars[r][0]);
     }
 
-    T y[kStates];
-    double lsc = 0.0;
+    T y[W][kStates];
+    double lsc[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) lsc[w] = 0.0;
     int prev = -1;
     bool ok = true;
     uint32_t phase = 0;
@@ -255,14 +290,20 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
         const int oi = c1prev ? 1 : 0;  // index of the "other" child (c1 when neither is prev)
         const int o = oi ? nj.c2 : nj.c1;
         const int fi = 1 - oi;          // index of the register / first child
-        double lsc_o = 0.0;
-        int code_o = 0;
+        double lsc_o[W];
+        int code_o[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) { lsc_o[w] = 0.0; code_o[w] = 0; }
         if (valid) {
             if (o >= d.T) {
                 const int wsc = (nj.ws >> (1 + oi)) & 1;
-                lsc_o = LSCp[(size_t)(o - d.T) * 2 * lws_stride + wsc * lws_stride + col];
+                const double* lp = LSCp + (size_t)(o - d.T) * 2 * lws_stride + wsc * lws_stride;
+#pragma unroll
+                for (int w = 0; w < W; ++w) lsc_o[w] = lp[col[w]];
             } else {
-                code_o = a.codes[(size_t)o * d.S + site];
+                const uint8_t* cp = a.codes + (size_t)o * d.S;
+#pragma unroll
+                for (int w = 0; w < W; ++w) code_o[w] = cp[site[w]];
             }
         }
         if (ok && !mbar_wait_bounded(&bars[r][b], (phase >> b) & 1)) {
@@ -273,75 +314,85 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
         if (ok && valid) {
             const T* Pf = buf + (size_t)(b * 2 + fi) * kPBlock;
             const T* Po = buf + (size_t)(b * 2 + oi) * kPBlock;
-            T acc[kStates];
-            double lsc_f = 0.0;
+            T acc[W][kStates];
+            double lsc_f[W];
             if (c1prev || c2prev) {
-                matvec(Pf, y, acc);
-                lsc_f = lsc;
+                matvec<T, W, false, RB>(Pf, y, acc);
+#pragma unroll
+                for (int w = 0; w < W; ++w) lsc_f[w] = lsc[w];
             } else {
                 // Neither child was just computed (both-tip nodes, or a list that
                 // is not a plain post-order): the first child comes from memory.
                 const int f = fi ? nj.c2 : nj.c1;
                 if (f >= d.T) {
                     const int wsf = (nj.ws >> (1 + fi)) & 1;
-                    const T* fp = CLp + (size_t)(f - d.T) * node_stride + wsf * ws_stride + col;
+                    const T* fp = CLp + (size_t)(f - d.T) * node_stride + wsf * ws_stride;
+                    const double* lp = LSCp + (size_t)(f - d.T) * 2 * lws_stride + wsf * lws_stride;
 #pragma unroll
-                    for (int j = 0; j < kStates; ++j) y[j] = fp[j * j_stride];
-                    lsc_f = LSCp[(size_t)(f - d.T) * 2 * lws_stride + wsf * lws_stride + col];
-                    matvec(Pf, y, acc);
+                    for (int w = 0; w < W; ++w) {
+#pragma unroll
+                        for (int j = 0; j < kStates; ++j) y[w][j] = fp[col[w] + j * j_stride];
+                        lsc_f[w] = lp[col[w]];
+                    }
+                    matvec<T, W, false, RB>(Pf, y, acc);
                 } else {
-                    const int code = a.codes[(size_t)f * d.S + site];
-                    const int cc = code < kStates ? code : kStates;
+                    const uint8_t* cp = a.codes + (size_t)f * d.S;
 #pragma unroll
-                    for (int i = 0; i < kStates; ++i) acc[i] = Pf[i * kPCols + cc];
+                    for (int w = 0; w < W; ++w) {
+                        const int code = cp[site[w]];
+                        const int cc = code < kStates ? code : kStates;
+#pragma unroll
+                        for (int i = 0; i < kStates; ++i) acc[w][i] = Pf[i * kPCols + cc];
+                        lsc_f[w] = 0.0;
+                    }
                 }
             }
             if (o >= d.T) {
                 // The register child is consumed; its registers now hold the
                 // other child's stored partial, folded in row by row.
                 const int wsc = (nj.ws >> (1 + oi)) & 1;
-                const T* xp = CLp + (size_t)(o - d.T) * node_stride + wsc * ws_stride + col;
+                const T* xp = CLp + (size_t)(o - d.T) * node_stride + wsc * ws_stride;
 #pragma unroll
-                for (int j = 0; j < kStates; ++j) y[j] = xp[j * j_stride];
+                for (int w = 0; w < W; ++w) {
 #pragma unroll
-                for (int i = 0; i < kStates; ++i) {
-                    const P2* row = reinterpret_cast<const P2*>(Po + i * kPCols);
-                    T s0 = 0, s1 = 0;
-#pragma unroll
-                    for (int j = 0; j < kStates / 2; ++j) {
-                        const P2 p2 = row[j];
-                        s0 = fma(p2.x, y[2 * j], s0);
-                        s1 = fma(p2.y, y[2 * j + 1], s1);
-                    }
-                    acc[i] *= s0 + s1;
+                    for (int j = 0; j < kStates; ++j) y[w][j] = xp[col[w] + j * j_stride];
                 }
+                matvec<T, W, true, RB>(Po, y, acc);
             } else {
-                const int cc = code_o < kStates ? code_o : kStates;
 #pragma unroll
-                for (int i = 0; i < kStates; ++i) acc[i] *= Po[i * kPCols + cc];
+                for (int w = 0; w < W; ++w) {
+                    const int cc = code_o[w] < kStates ? code_o[w] : kStates;
+#pragma unroll
+                    for (int i = 0; i < kStates; ++i) acc[w][i] *= Po[i * kPCols + cc];
+                }
             }
-            T mx = 0;
-#pragma unroll
-            for (int i = 0; i < kStates; ++i) mx = fmax(mx, acc[i]);
-            double l;
-            if (mx > 0) {
-                const int e = exponent_of(mx);
-                const T sc = pow2(mx, -e);
-#pragma unroll
-                for (int i = 0; i < kStates; ++i) acc[i] *= sc;
-                l = e * 0.69314718055994530942;
-            } else {
-                l = (mx == 0) ? -INFINITY : NAN;
-            }
-            lsc = l + lsc_f + lsc_o;
             const int wso = nj.ws & 1;
-            T* out = CLp + (size_t)(nj.node - d.T) * node_stride + wso * ws_stride + col;
+            T* out = CLp + (size_t)(nj.node - d.T) * node_stride + wso * ws_stride;
+            double* lout = LSCp + (size_t)(nj.node - d.T) * 2 * lws_stride + wso * lws_stride;
 #pragma unroll
-            for (int j = 0; j < kStates; ++j) {
-                y[j] = acc[j];
-                out[j * j_stride] = acc[j];
+            for (int w = 0; w < W; ++w) {
+                T mx = 0;
+#pragma unroll
+                for (int i = 0; i < kStates; ++i) mx = fmax(mx, acc[w][i]);
+                double l;
+                if (mx > 0) {
+                    const int e = exponent_of(mx);
+                    const T sc = pow2(mx, -e);
+#pragma unroll
+                    for (int i = 0; i < kStates; ++i) acc[w][i] *= sc;
+                    l = e * 0.69314718055994530942;
+                } else {
+                    l = (mx == 0) ? -INFINITY : NAN;
+                }
+                lsc[w] = l + lsc_f[w] + lsc_o[w];
+#pragma unroll
+                for (int j = 0; j < kStates; ++j) y[w][j] = acc[w][j];
+                if (vw[w]) {
+#pragma unroll
+                    for (int j = 0; j < kStates; ++j) out[col[w] + j * j_stride] = acc[w][j];
+                    lout[col[w]] = lsc[w];
+                }
             }
-            LSCp[(size_t)(nj.node - d.T) * 2 * lws_stride + wso * lws_stride + col] = lsc;
         }
         prev = nj.node;
         __syncwarp();
@@ -356,46 +407,58 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     }
     // Root reduction for this tile.
     if (cnt == 0 && valid) {
-        const T* xp = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride + col;
+        const T* xp = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride;
+        const double* lp = LSCp + (size_t)(h->root - d.T) * 2 * lws_stride + h->root_ws * lws_stride;
 #pragma unroll
-        for (int j = 0; j < kStates; ++j) y[j] = xp[j * j_stride];
-        lsc = LSCp[(size_t)(h->root - d.T) * 2 * lws_stride + h->root_ws * lws_stride + col];
+        for (int w = 0; w < W; ++w) {
+#pragma unroll
+            for (int j = 0; j < kStates; ++j) y[w][j] = xp[col[w] + j * j_stride];
+            lsc[w] = lp[col[w]];
+        }
     }
     const double* rec =
         a.spec + (((size_t)p * d.Kmax + tl.k) * 2 + a.sws[(size_t)p * d.Kmax + tl.k]) * kSpecStride;
     const double* pi = rec + kSpecPi;
     if (valid) {
-        double s = 0.0;
 #pragma unroll
-        for (int i = 0; i < kStates; ++i) s = fma(pi[i], (double)y[i], s);
-        red[r][lane] = log(s) + lsc;
+        for (int w = 0; w < W; ++w) {
+            double s = 0.0;
+#pragma unroll
+            for (int i = 0; i < kStates; ++i) s = fma(pi[i], (double)y[w][i], s);
+            red[r][lane + 32 * w] = log(s) + lsc[w];
+        }
     }
     __syncthreads();
     if (r == 0) {
         double v = 0.0;
-        if (valid) {
-            double mx = red[0][lane];
 #pragma unroll
-            for (int rr = 1; rr < R; ++rr) mx = fmax(mx, red[rr][lane]);
+        for (int w = 0; w < W; ++w) {
+            if (!vw[w]) continue;
+            const int q = lane + 32 * w;
+            double mx = red[0][q];
+#pragma unroll
+            for (int rr = 1; rr < R; ++rr) mx = fmax(mx, red[rr][q]);
             double lse = mx;
             if (mx > -INFINITY) {
                 double se = 0.0;
 #pragma unroll
-                for (int rr = 0; rr < R; ++rr) se += exp(red[rr][lane] - mx);
+                for (int rr = 0; rr < R; ++rr) se += exp(red[rr][q] - mx);
                 lse = mx + log(se);
             }
             // +I mixing, Particle.cpp:667-670, evaluated in log space.
             const double pinv = h->pinv;
-            if (pinv > 0.0 && a.isinv[site] != 0) {
+            double u;
+            if (pinv > 0.0 && a.isinv[site[w]] != 0) {
                 const double la = log1p(-pinv) + lse;
-                const double lb = log(pinv * pi[a.invchar[site]]);
+                const double lb = log(pinv * pi[a.invchar[site[w]]]);
                 const double m2 = fmax(la, lb);
-                v = m2 + log(exp(la - m2) + exp(lb - m2));
+                u = m2 + log(exp(la - m2) + exp(lb - m2));
             } else {
-                v = lse + log1p(-pinv);
+                u = lse + log1p(-pinv);
             }
-            if (bad) v = NAN;
-            a.site_lnl[(size_t)p * d.S + site] = v;
+            if (bad) u = NAN;
+            a.site_lnl[(size_t)p * d.S + site[w]] = u;
+            v += u;
         }
         v = warp_sum(v);
         if (lane == 0) a.partial[tile_id] = v;
@@ -440,50 +503,91 @@ cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, 
 
 namespace {
 
-template <class T, int R, int MINB>
+template <class T, int R, int MINB, int W, int RB>
 cudaError_t launch_prune_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
     const size_t smem = sizeof(T) * 4 * (size_t)kPBlock * R;
-    cudaError_t e = cudaFuncSetAttribute(prune_kernel<T, R, MINB>,
+    cudaError_t e = cudaFuncSetAttribute(prune_kernel<T, R, MINB, W, RB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    prune_kernel<T, R, MINB><<<ntiles, 32 * R, smem, st>>>(a);
+    prune_kernel<T, R, MINB, W, RB><<<ntiles, 32 * R, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+// SIMT variants as (sites per lane W, CTAs per SM MINB, mat-vec rows in flight RB):
+//   R = 4:  0 (1,4,1)  1 (1,3,1)  2 (1,2,1)  3 (1,3,4)  4 (1,4,4)  5 (1,2,4)  6 (2,2,1)
+//           FP32 only, where 40 registers hold a lane's two 20-vectors:
+//           7 (1,5,1)  8 (1,6,1)  9 (1,5,4)
+//   other:  0 (1,-,1)  1 (1,-,4)  2 (2,-,1)
+// W = 2 variants take 64-slot tiles, the others 32-slot tiles.
+int simt_variants(int R, bool fp32) { return R == 4 ? (fp32 ? 10 : 7) : 3; }
+int simt_width(int R, int v) { return (R == 4 ? v == 6 : v == 2) ? 2 : 1; }
+
+template <class T, int R, int MINB, int MINB2>
+cudaError_t launch_prune_r(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
+    switch (variant) {
+        case 1: return launch_prune_t<T, R, MINB, 1, 4>(a, ntiles, st);
+        case 2: return launch_prune_t<T, R, MINB2, 2, 1>(a, ntiles, st);
+        default: return launch_prune_t<T, R, MINB, 1, 1>(a, ntiles, st);
+    }
+}
+
+template <class T>
+cudaError_t launch_prune_r4(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
+    switch (variant) {
+        case 1: return launch_prune_t<T, 4, 3, 1, 1>(a, ntiles, st);
+        case 2: return launch_prune_t<T, 4, 2, 1, 1>(a, ntiles, st);
+        case 3: return launch_prune_t<T, 4, 3, 1, 4>(a, ntiles, st);
+        case 4: return launch_prune_t<T, 4, 4, 1, 4>(a, ntiles, st);
+        case 5: return launch_prune_t<T, 4, 2, 1, 4>(a, ntiles, st);
+        case 6: return launch_prune_t<T, 4, 2, 2, 1>(a, ntiles, st);
+        default: return launch_prune_t<T, 4, 4, 1, 1>(a, ntiles, st);
+    }
 }
 
 template <class T>
 cudaError_t launch_prune_typed(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
     switch (a.d.R) {
-        case 1: return launch_prune_t<T, 1, 4>(a, ntiles, st);
-        case 2: return launch_prune_t<T, 2, 4>(a, ntiles, st);
-        case 3: return launch_prune_t<T, 3, 4>(a, ntiles, st);
-        case 4:
-            if (variant == 1) return launch_prune_t<T, 4, 3>(a, ntiles, st);
-            if (variant == 2) return launch_prune_t<T, 4, 2>(a, ntiles, st);
-            return launch_prune_t<T, 4, 4>(a, ntiles, st);
-        case 5: return launch_prune_t<T, 5, 2>(a, ntiles, st);
-        case 6: return launch_prune_t<T, 6, 2>(a, ntiles, st);
-        case 7: return launch_prune_t<T, 7, 2>(a, ntiles, st);
-        case 8: return launch_prune_t<T, 8, 2>(a, ntiles, st);
+        case 1: return launch_prune_r<T, 1, 4, 8>(a, ntiles, variant, st);
+        case 2: return launch_prune_r<T, 2, 4, 4>(a, ntiles, variant, st);
+        case 3: return launch_prune_r<T, 3, 4, 2>(a, ntiles, variant, st);
+        case 4: return launch_prune_r4<T>(a, ntiles, variant, st);
+        case 5: return launch_prune_r<T, 5, 2, 1>(a, ntiles, variant, st);
+        case 6: return launch_prune_r<T, 6, 2, 1>(a, ntiles, variant, st);
+        case 7: return launch_prune_r<T, 7, 2, 1>(a, ntiles, variant, st);
+        case 8: return launch_prune_r<T, 8, 2, 1>(a, ntiles, variant, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
-}  // namespace
+cudaError_t launch_prune_fp32(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
+    if (a.d.R == 4) {
+        switch (variant) {
+            case 7: return launch_prune_t<float, 4, 5, 1, 1>(a, ntiles, st);
+            case 8: return launch_prune_t<float, 4, 6, 1, 1>(a, ntiles, st);
+            case 9: return launch_prune_t<float, 4, 5, 1, 4>(a, ntiles, st);
+            default: break;
+        }
+    }
+    return launch_prune_typed<float>(a, ntiles, variant, st);
+}
 
-namespace {
-int simt_variants(int R) { return R == 4 ? 3 : 1; }
 }  // namespace
 
 // FP64 contexts also have the tensor-path (DMMA) kernels, numbered after the
-// SIMT ones.
+// SIMT ones; they use 32-slot tiles.
 int prune_variants(int R, bool fp32) {
-    return simt_variants(R) + (fp32 ? 0 : prune_dmma_variants(R));
+    return simt_variants(R, fp32) + (fp32 ? 0 : prune_dmma_variants(R));
+}
+
+int prune_variant_tile_sites(int R, bool fp32, int variant) {
+    if (variant < simt_variants(R, fp32)) return 32 * simt_width(R, variant);
+    return 32;
 }
 
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
     if (ntiles <= 0) return cudaSuccess;
-    if (a.fp32) return launch_prune_typed<float>(a, ntiles, variant, st);
-    const int ns = simt_variants(a.d.R);
+    if (a.fp32) return launch_prune_fp32(a, ntiles, variant, st);
+    const int ns = simt_variants(a.d.R, false);
     if (variant >= ns) return launch_prune_dmma(a, ntiles, variant - ns, st);
     return launch_prune_typed<double>(a, ntiles, variant, st);
 }

@@ -440,7 +440,7 @@ class Engine:
     def autotune(self, reps: int = 3) -> dict:
         """Pick the fastest pruning-kernel variant on the loaded particles."""
         v = ctypes.c_int32(0)
-        ms = np.full(8, np.nan)
+        ms = np.full(self.kernel_variants()[0], np.nan)
         _check(lib().smccat_autotune(self._h, int(reps), ctypes.byref(v), ms.ctypes.data_as(_dp)))
         return {"variant": int(v.value), "ms": [float(x) for x in ms if not np.isnan(x)]}
 
