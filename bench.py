@@ -249,9 +249,15 @@ def measure_config_waves(cid, steps, local, rank, particles=0, oracle_sample=2):
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
+        eng.set_profiling(True)
+        one_pass()
+        prof = eng.profile()
+        eng.set_profiling(False)
         res[name] = {"value": n * cfg.S * cfg.R / (ms * 1e-3), "unit": UNIT, "ms_per_pass": ms,
                      "particles_per_wave": W, "waves": (n + W - 1) // W,
-                     "device_gb": eng.device_bytes / 1e9}
+                     "device_gb": eng.device_bytes / 1e9,
+                     "kernel_ms_per_pass": {k: round(v, 3) for k, v in prof["ms"].items()},
+                     "prune_variant": eng.kernel_variants()[1]}
         eng.close()
     d = np.abs(lnls["fp32"] - lnls["fp64"])
     res["fp32_vs_fp64_abs_dlogl"] = {"max": float(d.max()), "mean": float(d.mean())}

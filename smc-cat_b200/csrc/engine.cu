@@ -339,6 +339,7 @@ int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** o
     A(&c->d_tiles, (size_t)c->tile_cap);
     A(&c->d_tile_off, (size_t)P + 1);
     c->esz = (int)esz;
+    select_variant(c, prune_default_variant(d.R, esz == 4));
     A(&c->d_CL, cl * esz);
     A(&c->d_LSC, lsc);
     A(&c->d_Pm, pm * esz);
@@ -350,7 +351,9 @@ int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** o
     A(&c->d_site_lnl, (size_t)P * S);
     A(&c->d_status, 1);
     c->plan_cap = sizeof(PartHdr) * P + sizeof(NodeJob) * (size_t)P * d.NI +
-                  sizeof(PJob) * (size_t)P * N + sizeof(SpecJob) * (size_t)P * K + P + 64;
+                  sizeof(PJob) * (size_t)P * N +
+                  sizeof(PmJob) * (size_t)P * K * ((N + kPmChunk - 1) / kPmChunk) +
+                  sizeof(SpecJob) * (size_t)P * K + P + 64;
     A(&c->d_plan, c->plan_cap);
     if (rc != SMCCAT_OK) { smccat_destroy(c); return rc; }
     if (cudaMallocHost((void**)&c->h_plan, c->plan_cap) != cudaSuccess ||
@@ -551,21 +554,29 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
     off = (off + 15) & ~size_t(15);
     PJob* pjobs = reinterpret_cast<PJob*>(hp + off);
     const size_t pjob_off = off;
-    int np_ = 0;
+    int np_ = 0, nm = 0;
     for (int i = 0; i < count; ++i) {
         const Slot& s = c->slots[first + i];
         if (!on(i)) continue;
         const bool full = (mode == SMCCAT_REFRESH_FULL) || s.full;
-        if (full) np_ += N - 1;
-        else for (int n = 0; n < N; ++n) np_ += (s.dirty_p[n] && n != s.cur.root);
+        int np_i = 0;
+        if (full) np_i = N - 1;
+        else for (int n = 0; n < N; ++n) np_i += (s.dirty_p[n] && n != s.cur.root);
+        np_ += np_i;
+        nm += s.cur.K * ((np_i + kPmChunk - 1) / kPmChunk);
     }
     off += sizeof(PJob) * np_;
+    off = (off + 15) & ~size_t(15);
+    PmJob* mjobs = reinterpret_cast<PmJob*>(hp + off);
+    const size_t mjob_off = off;
+    off += sizeof(PmJob) * nm;
     off = (off + 15) & ~size_t(15);
     SpecJob* sjobs = reinterpret_cast<SpecJob*>(hp + off);
     const size_t sjob_off = off;
     int ns = 0;
     nn = 0;
     np_ = 0;
+    nm = 0;
     for (int i = 0; i < count; ++i) {
         const int p = first + i;
         Slot& s = c->slots[p];
@@ -590,11 +601,15 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
             std::memcpy(j.base, m.base.data(), sizeof(j.base));
             std::memcpy(j.logits, &m.logits[(size_t)k * kStates], sizeof(j.logits));
         }
+        const int pj0 = np_;
         for (int n = 0; n < N; ++n) {
             if (!s.dirty_p[n] || n == m.root) continue;
             m.pws[n] = 1 - s.old.pws[n];
             pjobs[np_++] = PJob{p, n, m.pws[n], 0, m.branch[n]};
         }
+        for (int k = 0; k < m.K; ++k)
+            for (int q = pj0; q < np_; q += kPmChunk)
+                mjobs[nm++] = PmJob{i, k, q, std::min(kPmChunk, np_ - q)};
         PartHdr& h = hdr[i];
         h.node_off = nn;
         for (int n : m.post) {
@@ -637,7 +652,8 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
         }));
     if (np_ > 0)
         CK(launch(c, SMCCAT_KERNEL_PMAT, [&] {
-            return launch_pmat(reinterpret_cast<const PJob*>(c->d_plan + pjob_off), np_, d_hdr, first,
+            return launch_pmat(reinterpret_cast<const PmJob*>(c->d_plan + mjob_off), nm,
+                               reinterpret_cast<const PJob*>(c->d_plan + pjob_off), d_hdr, first,
                                c->d_sws, c->d_spec, c->d_Pm, c->esz == 4, d, c->st);
         }));
     PruneArgs a{};

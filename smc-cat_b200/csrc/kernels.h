@@ -34,13 +34,17 @@ struct PruneArgs {
 };
 
 cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d, cudaStream_t st);
-cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, const uint8_t* sws,
-                        const double* spec, void* Pm, bool fp32, const Dims& d, cudaStream_t st);
+cudaError_t launch_pmat(const PmJob* mjobs, int n, const PJob* jobs, const PartHdr* hdr, int first,
+                        const uint8_t* sws, const double* spec, void* Pm, bool fp32, const Dims& d,
+                        cudaStream_t st);
 // Pruning kernel variants available for R rate categories: SIMT kernels at
 // several register caps, then (FP64 only) the FP64 tensor-path kernels.
 int prune_variants(int R, bool fp32);
 // Slots per pruning tile that a variant expects (32 or 64).
 int prune_variant_tile_sites(int R, bool fp32, int variant);
+// The variant used until smccat_autotune or smccat_set_kernel_variant picks
+// another: the fastest measured on B200 for the bench workloads.
+int prune_default_variant(int R, bool fp32);
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
 int prune_dmma_variants(int R);
 cudaError_t launch_prune_dmma(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);

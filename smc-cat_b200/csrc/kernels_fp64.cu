@@ -2,15 +2,17 @@
 //
 //   spec_kernel   one warp per (particle, class): spectral decomposition of the
 //                 class's rate matrix (spectral.cuh).
-//   pmat_kernel   one CTA per (particle, node): P(t r) = L diag(exp(lambda t r)) Rm
-//                 for every class and rate (TransitionProbabilityClass.cpp:83-95),
-//                 row-major with a row-sum column.
+//   pmat_kernel   one CTA per (particle, class, chunk of dirty nodes):
+//                 P(t r) = L diag(exp(lambda t r)) Rm for every rate
+//                 (TransitionProbabilityClass.cpp:83-95), row-major with a
+//                 row-sum column, register-tiled.
 //   prune_kernel  one warp per (rate, tile of <= 32 W same-class sites, W sites
 //                 per lane), R warps per CTA: walks the particle's dirty
 //                 internal nodes in post-order (Particle.cpp:577-626). Each warp
-//                 stages its two children's P blocks into shared memory with TMA bulk copies (double-buffered,
-//                 mbarrier-tracked, the next node's copy in flight while the
-//                 current node computes), keeps the partial it just produced in
+//                 stages its two children's P blocks into shared memory with TMA
+//                 bulk copies (double-buffered, mbarrier-tracked, the next node's
+//                 copy in flight while the current node computes), keeps the
+//                 partial it just produced in
 //                 registers (in a post-order of an upward-closed dirty set the
 //                 previous node is always a child of the next one), reads at most
 //                 one child partial back from memory, rescales each (site, rate)
@@ -90,6 +92,17 @@ __device__ __forceinline__ int exponent_of(float mx) { int e; frexpf(mx, &e); re
 __device__ __forceinline__ double pow2(double, int e) { return ldexp(1.0, e); }
 __device__ __forceinline__ float pow2(float, int e) { return ldexpf(1.0f, e); }
 
+// max(0, v[0..19]) as a depth-5 tree instead of a 20-long dependent chain.
+template <class T>
+__device__ __forceinline__ T max20(const T* v) {
+    T m[10];
+#pragma unroll
+    for (int i = 0; i < 10; ++i) m[i] = fmax(v[2 * i], v[2 * i + 1]);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) m[i] = fmax(m[2 * i], m[2 * i + 1]);
+    return fmax(fmax(fmax(m[0], m[1]), fmax(m[2], m[3])), fmax(m[4], T(0)));
+}
+
 // acc[w][i] = sum_j P[i][j] x[w][j] for the W sites of a lane, P row-major
 // (stride kPCols) in shared memory, every lane reading the same element.
 // MUL: multiply the result into acc instead of assigning it.
@@ -143,54 +156,86 @@ __global__ void __launch_bounds__(32) spec_kernel(const SpecJob* __restrict__ jo
 }
 
 // ---------------------------------------------------------------------------
-// Transition matrices of one node for every class and rate.
+// Transition matrices of one class for a chunk of a particle's dirty nodes,
+// every rate: P(t r) = (L diag(exp(lambda t r))) [Rm | Rm 1] with a 21st
+// column of row sums and a zero pad column. The class's eigensystem is staged
+// in shared memory once per CTA; each thread owns a 4 x 4 output tile of one
+// rate (5 row blocks x 6 column blocks x R rates), so every shared-memory load
+// feeds several FMAs. Summation order over m is that of the plain triple loop.
 // Computed in FP64; stored as T (rounded once for the FP32 path).
+constexpr int kPmThreads = 128;
 template <class T>
-__global__ void __launch_bounds__(128) pmat_kernel(const PJob* __restrict__ jobs,
-                                                   const PartHdr* __restrict__ hdr, int first,
-                                                   const uint8_t* __restrict__ sws,
-                                                   const double* __restrict__ spec,
-                                                   T* __restrict__ Pm, Dims d) {
-    const PJob job = jobs[blockIdx.x];
-    const PartHdr* h = hdr + (job.p - first);
-    __shared__ double L[kStates][kStates + 1];
-    __shared__ double Rm[kStates][kStates + 1];
-    __shared__ double ex[kMaxRates][kStates];
-    __shared__ double rs[kStates];
+__global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restrict__ mjobs,
+                                                          const PJob* __restrict__ jobs,
+                                                          const PartHdr* __restrict__ hdr, int first,
+                                                          const uint8_t* __restrict__ sws,
+                                                          const double* __restrict__ spec,
+                                                          T* __restrict__ Pm, Dims d) {
+    const PmJob mj = mjobs[blockIdx.x];
+    const PartHdr* h = hdr + mj.i;
+    const int p = first + mj.i;
+    __shared__ __align__(16) double Lt[kStates][kStates];  // Lt[m][i] = L[i][m]
+    __shared__ __align__(16) double Rx[kStates][24];       // Rm | row sums | zeros
+    __shared__ double lam[kStates];
+    __shared__ double ex[2][kMaxRates][kStates];
     const int tid = threadIdx.x;
-    for (int k = 0; k < h->num_classes; ++k) {
-        const double* rec =
-            spec + (((size_t)job.p * d.Kmax + k) * 2 + sws[(size_t)job.p * d.Kmax + k]) * kSpecStride;
+    const double* rec =
+        spec + (((size_t)p * d.Kmax + mj.k) * 2 + sws[(size_t)p * d.Kmax + mj.k]) * kSpecStride;
+    for (int idx = tid; idx < kStates * kStates; idx += kPmThreads) {
+        const int a = idx / kStates, b = idx % kStates;
+        Lt[b][a] = rec[kSpecL + idx];
+        Rx[a][b] = rec[kSpecRm + idx];
+    }
+    if (tid < kStates) {
+        double s = 0.0;
+        for (int j = 0; j < kStates; ++j) s += rec[kSpecRm + tid * kStates + j];
+        Rx[tid][kStates] = s;
+        Rx[tid][21] = Rx[tid][22] = Rx[tid][23] = 0.0;
+        lam[tid] = rec[kSpecLam + tid];
+    }
+    const int ntile = 30 * d.R;
+    for (int q = 0; q < mj.nj; ++q) {
+        const PJob pj = jobs[mj.j0 + q];
+        const int b = q & 1;  // ex double buffer: one barrier per node
         __syncthreads();
-        for (int idx = tid; idx < kStates * kStates; idx += blockDim.x) {
-            L[idx / kStates][idx % kStates] = rec[kSpecL + idx];
-            Rm[idx / kStates][idx % kStates] = rec[kSpecRm + idx];
-        }
-        for (int idx = tid; idx < d.R * kStates; idx += blockDim.x) {
+        for (int idx = tid; idx < d.R * kStates; idx += kPmThreads) {
             const int r = idx / kStates, m = idx % kStates;
-            ex[r][m] = exp(rec[kSpecLam + m] * job.t * h->rates[r]);
+            ex[b][r][m] = exp(lam[m] * pj.t * h->rates[r]);
         }
         __syncthreads();
-        if (tid < kStates) {
-            double s = 0.0;
-            for (int j = 0; j < kStates; ++j) s += Rm[tid][j];
-            rs[tid] = s;
-        }
-        __syncthreads();
-        T* out = Pm + ((((size_t)job.p * d.Kmax + k) * d.N + job.node) * 2 + job.pws) *
+        T* out = Pm + ((((size_t)p * d.Kmax + mj.k) * d.N + pj.node) * 2 + pj.pws) *
                           (size_t)d.R * kPBlock;
-        for (int idx = tid; idx < d.R * kPBlock; idx += blockDim.x) {
-            const int r = idx / kPBlock, e = idx % kPBlock;
-            const int i = e / kPCols, j = e % kPCols;
-            double v = 0.0;
-            if (j < kStates) {
+        for (int t = tid; t < ntile; t += kPmThreads) {
+            const int r = t / 30, i0 = 4 * ((t % 30) / 6), j0 = 4 * (t % 6);
+            double acc[4][4];
 #pragma unroll
-                for (int m = 0; m < kStates; ++m) v = fma(L[i][m] * ex[r][m], Rm[m][j], v);
-            } else if (j == kStates) {
+            for (int u = 0; u < 4; ++u) {
 #pragma unroll
-                for (int m = 0; m < kStates; ++m) v = fma(L[i][m] * ex[r][m], rs[m], v);
+                for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
             }
-            out[idx] = static_cast<T>(v);
+#pragma unroll 4
+            for (int m = 0; m < kStates; ++m) {
+                const double e = ex[b][r][m];
+                const double2 a01 = *reinterpret_cast<const double2*>(&Lt[m][i0]);
+                const double2 a23 = *reinterpret_cast<const double2*>(&Lt[m][i0 + 2]);
+                const double2 b01 = *reinterpret_cast<const double2*>(&Rx[m][j0]);
+                const double2 b23 = *reinterpret_cast<const double2*>(&Rx[m][j0 + 2]);
+                const double av[4] = {a01.x * e, a01.y * e, a23.x * e, a23.y * e};
+                const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+                }
+            }
+            T* o = out + (size_t)r * kPBlock;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    if (j0 + v < kPCols) o[(i0 + u) * kPCols + j0 + v] = static_cast<T>(acc[u][v]);
+                }
+            }
         }
     }
 }
@@ -371,9 +416,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
             double* lout = LSCp + (size_t)(nj.node - d.T) * 2 * lws_stride + wso * lws_stride;
 #pragma unroll
             for (int w = 0; w < W; ++w) {
-                T mx = 0;
-#pragma unroll
-                for (int i = 0; i < kStates; ++i) mx = fmax(mx, acc[w][i]);
+                const T mx = max20(acc[w]);
                 double l;
                 if (mx > 0) {
                     const int e = exponent_of(mx);
@@ -493,11 +536,16 @@ cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d,
     return cudaGetLastError();
 }
 
-cudaError_t launch_pmat(const PJob* jobs, int n, const PartHdr* hdr, int first, const uint8_t* sws,
-                        const double* spec, void* Pm, bool fp32, const Dims& d, cudaStream_t st) {
+cudaError_t launch_pmat(const PmJob* mjobs, int n, const PJob* jobs, const PartHdr* hdr, int first,
+                        const uint8_t* sws, const double* spec, void* Pm, bool fp32, const Dims& d,
+                        cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    if (fp32) pmat_kernel<float><<<n, 128, 0, st>>>(jobs, hdr, first, sws, spec, static_cast<float*>(Pm), d);
-    else pmat_kernel<double><<<n, 128, 0, st>>>(jobs, hdr, first, sws, spec, static_cast<double*>(Pm), d);
+    if (fp32)
+        pmat_kernel<float><<<n, kPmThreads, 0, st>>>(mjobs, jobs, hdr, first, sws, spec,
+                                                     static_cast<float*>(Pm), d);
+    else
+        pmat_kernel<double><<<n, kPmThreads, 0, st>>>(mjobs, jobs, hdr, first, sws, spec,
+                                                      static_cast<double*>(Pm), d);
     return cudaGetLastError();
 }
 
@@ -577,6 +625,14 @@ cudaError_t launch_prune_fp32(const PruneArgs& a, int ntiles, int variant, cudaS
 // SIMT ones; they use 32-slot tiles.
 int prune_variants(int R, bool fp32) {
     return simt_variants(R, fp32) + (fp32 ? 0 : prune_dmma_variants(R));
+}
+
+// FP64: one site per lane, four rows in flight (variant 3 at R = 4: 6.76 ms
+// against 7.07 ms for one row in flight, 48 taxa x 2,000 sites x 256
+// particles). FP32: the 128-register one-row variant.
+int prune_default_variant(int R, bool fp32) {
+    if (fp32) return 0;
+    return R == 4 ? 3 : 1;
 }
 
 int prune_variant_tile_sites(int R, bool fp32, int variant) {

@@ -64,6 +64,13 @@ struct PJob {
     double t;           // branch length
 };
 
+// One transition-matrix CTA: class k of plan particle i, for the PJobs
+// [j0, j0 + nj) of that particle (at most kPmChunk nodes).
+constexpr int kPmChunk = 16;
+struct PmJob {
+    int32_t i, k, j0, nj;
+};
+
 // Re-decompose one class.
 struct SpecJob {
     int32_t p, k, sws, pad;
