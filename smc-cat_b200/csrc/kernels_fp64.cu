@@ -177,7 +177,8 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
     __shared__ __align__(16) double Lt[kStates][kStates];  // Lt[m][i] = L[i][m]
     __shared__ __align__(16) double Rx[kStates][24];       // Rm | row sums | zeros
     __shared__ double lam[kStates];
-    __shared__ double ex[2][kMaxRates][kStates];
+    __shared__ double ex[kPmChunk][kMaxRates][kStates];
+    __shared__ size_t obase[kPmChunk];
     const int tid = threadIdx.x;
     const double* rec =
         spec + (((size_t)p * d.Kmax + mj.k) * 2 + sws[(size_t)p * d.Kmax + mj.k]) * kSpecStride;
@@ -193,20 +194,23 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
         Rx[tid][21] = Rx[tid][22] = Rx[tid][23] = 0.0;
         lam[tid] = rec[kSpecLam + tid];
     }
+    if (tid < mj.nj) {
+        const PJob pj = jobs[mj.j0 + tid];
+        obase[tid] = ((((size_t)p * d.Kmax + mj.k) * d.N + pj.node) * 2 + pj.pws) * (size_t)d.R * kPBlock;
+    }
+    __syncthreads();
+    // Every exponential of the chunk in one phase, then no barrier per node.
+    const int per_node = d.R * kStates;
+    for (int idx = tid; idx < mj.nj * per_node; idx += kPmThreads) {
+        const int q = idx / per_node, r = (idx % per_node) / kStates, m = idx % kStates;
+        ex[q][r][m] = exp(lam[m] * jobs[mj.j0 + q].t * h->rates[r]);
+    }
+    __syncthreads();
+    using P2 = typename Pair<T>::type;
     const int ntile = 30 * d.R;
-    for (int q = 0; q < mj.nj; ++q) {
-        const PJob pj = jobs[mj.j0 + q];
-        const int b = q & 1;  // ex double buffer: one barrier per node
-        __syncthreads();
-        for (int idx = tid; idx < d.R * kStates; idx += kPmThreads) {
-            const int r = idx / kStates, m = idx % kStates;
-            ex[b][r][m] = exp(lam[m] * pj.t * h->rates[r]);
-        }
-        __syncthreads();
-        T* out = Pm + ((((size_t)p * d.Kmax + mj.k) * d.N + pj.node) * 2 + pj.pws) *
-                          (size_t)d.R * kPBlock;
-        for (int t = tid; t < ntile; t += kPmThreads) {
-            const int r = t / 30, i0 = 4 * ((t % 30) / 6), j0 = 4 * (t % 6);
+    for (int t = tid; t < ntile; t += kPmThreads) {
+        const int r = t / 30, i0 = 4 * ((t % 30) / 6), j0 = 4 * (t % 6);
+        for (int q = 0; q < mj.nj; ++q) {
             double acc[4][4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -215,7 +219,7 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
             }
 #pragma unroll 4
             for (int m = 0; m < kStates; ++m) {
-                const double e = ex[b][r][m];
+                const double e = ex[q][r][m];
                 const double2 a01 = *reinterpret_cast<const double2*>(&Lt[m][i0]);
                 const double2 a23 = *reinterpret_cast<const double2*>(&Lt[m][i0 + 2]);
                 const double2 b01 = *reinterpret_cast<const double2*>(&Rx[m][j0]);
@@ -228,13 +232,13 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
                     for (int v = 0; v < 4; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
                 }
             }
-            T* o = out + (size_t)r * kPBlock;
+            // Pair stores: row offsets and j0 are even, so every pair is aligned.
+            T* o = Pm + obase[q] + (size_t)r * kPBlock + j0;
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    if (j0 + v < kPCols) o[(i0 + u) * kPCols + j0 + v] = static_cast<T>(acc[u][v]);
-                }
+                P2* row = reinterpret_cast<P2*>(o + (i0 + u) * kPCols);
+                row[0] = P2{static_cast<T>(acc[u][0]), static_cast<T>(acc[u][1])};
+                if (j0 + 4 <= kPCols) row[1] = P2{static_cast<T>(acc[u][2]), static_cast<T>(acc[u][3])};
             }
         }
     }
