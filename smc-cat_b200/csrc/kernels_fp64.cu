@@ -164,6 +164,11 @@ __global__ void __launch_bounds__(32) spec_kernel(const SpecJob* __restrict__ jo
 // feeds several FMAs. Summation order over m is that of the plain triple loop.
 // Computed in FP64; stored as T (rounded once for the FP32 path).
 constexpr int kPmThreads = 128;
+// Position of column c in a row of nb 4-column blocks stored as [half][block][2]:
+// the first pairs of all blocks, then the second pairs.
+__device__ __forceinline__ int pm_ilv(int c, int nb) {
+    return (((c >> 1) & 1) * nb + (c >> 2)) * 2 + (c & 1);
+}
 template <class T>
 __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restrict__ mjobs,
                                                           const PJob* __restrict__ jobs,
@@ -174,7 +179,9 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
     const PmJob mj = mjobs[blockIdx.x];
     const PartHdr* h = hdr + mj.i;
     const int p = first + mj.i;
-    __shared__ __align__(16) double Lt[kStates][kStates];  // Lt[m][i] = L[i][m]
+    // Rows in 4-column-block interleaved order (pm_ilv): the pair loads of a
+    // warp's tiles fall on distinct banks.
+    __shared__ __align__(16) double Lt[kStates][kStates];  // Lt[m][ilv(i)] = L[i][m]
     __shared__ __align__(16) double Rx[kStates][24];       // Rm | row sums | zeros
     __shared__ double lam[kStates];
     __shared__ double ex[kPmChunk][kMaxRates][kStates];
@@ -184,14 +191,14 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
         spec + (((size_t)p * d.Kmax + mj.k) * 2 + sws[(size_t)p * d.Kmax + mj.k]) * kSpecStride;
     for (int idx = tid; idx < kStates * kStates; idx += kPmThreads) {
         const int a = idx / kStates, b = idx % kStates;
-        Lt[b][a] = rec[kSpecL + idx];
-        Rx[a][b] = rec[kSpecRm + idx];
+        Lt[b][pm_ilv(a, 5)] = rec[kSpecL + idx];
+        Rx[a][pm_ilv(b, 6)] = rec[kSpecRm + idx];
     }
     if (tid < kStates) {
         double s = 0.0;
         for (int j = 0; j < kStates; ++j) s += rec[kSpecRm + tid * kStates + j];
-        Rx[tid][kStates] = s;
-        Rx[tid][21] = Rx[tid][22] = Rx[tid][23] = 0.0;
+        Rx[tid][pm_ilv(kStates, 6)] = s;
+        Rx[tid][pm_ilv(21, 6)] = Rx[tid][pm_ilv(22, 6)] = Rx[tid][pm_ilv(23, 6)] = 0.0;
         lam[tid] = rec[kSpecLam + tid];
     }
     if (tid < mj.nj) {
@@ -220,10 +227,10 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
 #pragma unroll 4
             for (int m = 0; m < kStates; ++m) {
                 const double e = ex[q][r][m];
-                const double2 a01 = *reinterpret_cast<const double2*>(&Lt[m][i0]);
-                const double2 a23 = *reinterpret_cast<const double2*>(&Lt[m][i0 + 2]);
-                const double2 b01 = *reinterpret_cast<const double2*>(&Rx[m][j0]);
-                const double2 b23 = *reinterpret_cast<const double2*>(&Rx[m][j0 + 2]);
+                const double2 a01 = *reinterpret_cast<const double2*>(&Lt[m][pm_ilv(i0, 5)]);
+                const double2 a23 = *reinterpret_cast<const double2*>(&Lt[m][pm_ilv(i0 + 2, 5)]);
+                const double2 b01 = *reinterpret_cast<const double2*>(&Rx[m][pm_ilv(j0, 6)]);
+                const double2 b23 = *reinterpret_cast<const double2*>(&Rx[m][pm_ilv(j0 + 2, 6)]);
                 const double av[4] = {a01.x * e, a01.y * e, a23.x * e, a23.y * e};
                 const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
