@@ -488,6 +488,10 @@ def main():
         except Exception:
             fp64_peak = None
         fp64_achieved = f_unit * units_per_step / (prune_ms * 1e-3) / 1e12
+        # Executed: a tip child costs a shared-memory gather, not a mat-vec, so
+        # only the T-2 internal child edges run 20x20 mat-vecs.
+        f_exec = (cfg.T - 2) * 800 + (cfg.T - 1) * 60
+        fp64_executed = f_exec * units_per_step / (prune_ms * 1e-3) / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -511,7 +515,10 @@ def main():
                          "min_bytes_frac": b_min * units_per_step / (prune_ms * 1e-3) / 1e9 / peak,
                          "avg_launch_ms": prune_ms},
             "fp64": {"achieved_tflops": fp64_achieved, "dgemm_peak_tflops": fp64_peak,
-                     "frac": (fp64_achieved / fp64_peak) if fp64_peak else None},
+                     "frac": (fp64_achieved / fp64_peak) if fp64_peak else None,
+                     "flops_per_unit": f_unit,
+                     "executed_flops_per_unit": f_exec, "executed_tflops": fp64_executed,
+                     "executed_frac": (fp64_executed / fp64_peak) if fp64_peak else None},
             "kernel_ms_per_step": {k: v / args.steps for k, v in prof["ms"].items()},
             "gpu_launches": sum(prof["launches"].values()),
             "mixed_precision": mixed,
