@@ -382,16 +382,18 @@ typedef struct smccat_profile {
     uint64_t d2h_bytes;                     /* device->host bytes copied        */
 } smccat_profile;
 
-/* Time every instantiated pruning-kernel variant (register caps / CTAs per
- * SM) with `reps` full refreshes of the loaded particles [0, n) and keep the
- * fastest for this context. Writes the chosen variant and, if ms_out is not
- * NULL, the per-variant pruning time (ms) for each variant (at most 8). The
+/* Time every instantiated pruning-kernel variant (sites per lane, mat-vec
+ * schedule, register cap) with `reps` full refreshes of the loaded particles
+ * [0, n) and keep the fastest for this context. Writes the chosen variant and,
+ * if ms_out is not NULL, the pruning time (ms) of each variant: ms_out needs
+ * one entry per variant, as many as smccat_kernel_variants reports. The
  * particles must have no pending edits; their likelihoods are recomputed. */
 int smccat_autotune(smccat_ctx* ctx, int32_t reps, int32_t* variant_out, double* ms_out);
 
-/* Number of pruning-kernel variants of this context (FP64 contexts: SIMT
- * kernels at three register caps, then FP64 tensor-path kernels), the one in
- * use, and a way to pin one (what smccat_autotune sets). */
+/* Number of pruning-kernel variants of this context (SIMT kernels of several
+ * schedules and register caps; FP64 contexts then add FP64 tensor-path
+ * kernels), the one in use, and a way to pin one (what smccat_autotune
+ * sets). A new context starts on the variant measured fastest on B200. */
 int smccat_kernel_variants(smccat_ctx* ctx, int32_t* count, int32_t* current);
 int smccat_set_kernel_variant(smccat_ctx* ctx, int32_t variant);
 
