@@ -11,6 +11,7 @@
 // restores the committed state by resetting host-side indices only
 // (the reference copies whole buffers, Particle.cpp:343-478).
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include <algorithm>
 #include <cmath>
@@ -88,6 +89,8 @@ struct smccat_ctx {
     std::vector<int32_t> tile_off;
     bool tiles_dirty = false;
     int32_t* h_perm = nullptr;  // pinned staging for slot -> site maps
+    Tile* h_tiles = nullptr;      // pinned staging for the tile list
+    int32_t* h_tile_off = nullptr;
     std::vector<int> perm_dirty;
 
     // measurement
@@ -214,17 +217,17 @@ cudaError_t launch(smccat_ctx* c, int kind, F&& f) {
     return e;
 }
 
-// Sites grouped by class (stable), then cut into tiles of <= tile_sites.
+// Sites grouped by class (stable), then cut into tiles of <= tile_sites; the
+// per-class site counts come from the last state upload.
 void rebuild_tiles(smccat_ctx* c) {
-    const int P = c->cfg.max_particles, S = c->d.S, ts = c->tile_sites;
+    const int P = c->cfg.max_particles, ts = c->tile_sites;
     c->tiles.clear();
     c->tile_off.assign(P + 1, 0);
     for (int p = 0; p < P; ++p) {
         c->tile_off[p] = (int)c->tiles.size();
         const Slot& s = c->slots[p];
         if (!s.loaded) continue;
-        std::vector<int> cnt(s.cur.K, 0);
-        for (int i = 0; i < S; ++i) cnt[s.assign[i]]++;
+        const std::vector<int32_t>& cnt = s.class_cnt;
         int slot0 = 0;
         for (int k = 0; k < s.cur.K; ++k) {
             for (int off = 0; off < cnt[k]; off += ts)
@@ -281,6 +284,8 @@ int smccat_destroy(smccat_ctx* c) {
     if (c->h_plan) cudaFreeHost(c->h_plan);
     if (c->h_sws) cudaFreeHost(c->h_sws);
     if (c->h_perm) cudaFreeHost(c->h_perm);
+    if (c->h_tiles) cudaFreeHost(c->h_tiles);
+    if (c->h_tile_off) cudaFreeHost(c->h_tile_off);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->plan_done) cudaEventDestroy(c->plan_done);
     if (c->st) cudaStreamDestroy(c->st);
@@ -358,7 +363,9 @@ int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** o
     if (rc != SMCCAT_OK) { smccat_destroy(c); return rc; }
     if (cudaMallocHost((void**)&c->h_plan, c->plan_cap) != cudaSuccess ||
         cudaMallocHost((void**)&c->h_sws, (size_t)P * K) != cudaSuccess ||
-        cudaMallocHost((void**)&c->h_perm, (size_t)P * S * sizeof(int32_t)) != cudaSuccess) {
+        cudaMallocHost((void**)&c->h_perm, (size_t)P * S * sizeof(int32_t)) != cudaSuccess ||
+        cudaMallocHost((void**)&c->h_tiles, (size_t)c->tile_cap * sizeof(Tile)) != cudaSuccess ||
+        cudaMallocHost((void**)&c->h_tile_off, ((size_t)P + 1) * sizeof(int32_t)) != cudaSuccess) {
         smccat_destroy(c);
         return fail(SMCCAT_ENOMEM, "pinned host allocation failed");
     }
@@ -422,31 +429,46 @@ int smccat_set_particles(smccat_ctx* c, int32_t first, int32_t count, const int3
         return fail(SMCCAT_EINVAL, "null argument");
     const Dims& d = c->d;
     const int N = d.N, S = d.S, Kmax = d.Kmax;
-    // Validate everything before touching any slot.
+    // Validate everything before touching any slot (particles in parallel;
+    // the first bad particle in index order is reported).
     std::vector<Mirror> trees(count);
+    std::vector<uint8_t> bad(count, 0);
+#pragma omp parallel for schedule(static) if (count >= kParallelParticles)
     for (int i = 0; i < count; ++i) {
-        if (!build_tree(d.T, parent + (size_t)i * N, &trees[i]))
-            return fail(SMCCAT_EINVAL, "particle " + std::to_string(first + i) + ": not a rooted binary tree");
+        uint8_t why = 0;
         const int K = num_classes[i];
-        if (K < 1 || K > Kmax)
-            return fail(SMCCAT_EINVAL, "particle " + std::to_string(first + i) + ": num_classes out of range");
-        if (!(c->cfg.model_flags & SMCCAT_MODEL_CAT) && K != 1)
-            return fail(SMCCAT_EINVAL, "num_classes must be 1 without SMCCAT_MODEL_CAT");
-        for (int s = 0; s < S; ++s) {
+        if (!build_tree(d.T, parent + (size_t)i * N, &trees[i])) why = 1;
+        else if (K < 1 || K > Kmax) why = 2;
+        else if (!(c->cfg.model_flags & SMCCAT_MODEL_CAT) && K != 1) why = 3;
+        for (int s = 0; s < S && !why; ++s) {
             const int k = assign[(size_t)i * S + s];
-            if (k < 0 || k >= K)
-                return fail(SMCCAT_EINVAL, "particle " + std::to_string(first + i) + ": class index out of range");
+            if (k < 0 || k >= K) why = 4;
         }
         const double pv = pinv[i];
-        if (!(pv >= 0.0 && pv < 1.0)) return fail(SMCCAT_EINVAL, "pinv must be in [0, 1)");
-        if (d.R > 1 && !(shape[i] > 0.0)) return fail(SMCCAT_EINVAL, "shape must be > 0");
-        for (int n = 0; n < N; ++n) {
+        if (!why && !(pv >= 0.0 && pv < 1.0)) why = 5;
+        if (!why && d.R > 1 && !(shape[i] > 0.0)) why = 6;
+        for (int n = 0; n < N && !why; ++n) {
             const double b = branch[(size_t)i * N + n];
-            if (!(b >= 0.0) || !std::isfinite(b)) return fail(SMCCAT_EINVAL, "branch lengths must be finite and >= 0");
+            if (!(b >= 0.0) || !std::isfinite(b)) why = 7;
+        }
+        bad[i] = why;
+    }
+    for (int i = 0; i < count; ++i) {
+        const std::string who = "particle " + std::to_string(first + i) + ": ";
+        switch (bad[i]) {
+            case 0: continue;
+            case 1: return fail(SMCCAT_EINVAL, who + "not a rooted binary tree");
+            case 2: return fail(SMCCAT_EINVAL, who + "num_classes out of range");
+            case 3: return fail(SMCCAT_EINVAL, "num_classes must be 1 without SMCCAT_MODEL_CAT");
+            case 4: return fail(SMCCAT_EINVAL, who + "class index out of range");
+            case 5: return fail(SMCCAT_EINVAL, "pinv must be in [0, 1)");
+            case 6: return fail(SMCCAT_EINVAL, "shape must be > 0");
+            default: return fail(SMCCAT_EINVAL, "branch lengths must be finite and >= 0");
         }
     }
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaEventSynchronize(c->plan_done));  // h_perm may still be in flight
+#pragma omp parallel for schedule(static) if (count >= kParallelParticles)
     for (int i = 0; i < count; ++i) {
         const int p = first + i;
         Slot& s = c->slots[p];
@@ -474,6 +496,7 @@ int smccat_set_particles(smccat_ctx* c, int32_t first, int32_t count, const int3
         int32_t* perm = c->h_perm + (size_t)p * S;
         std::vector<int> cnt(m.K + 1, 0);
         for (int x = 0; x < S; ++x) cnt[s.assign[x] + 1]++;
+        s.class_cnt.assign(cnt.begin() + 1, cnt.end());
         for (int k = 0; k < m.K; ++k) cnt[k + 1] += cnt[k];
         for (int x = 0; x < S; ++x) perm[cnt[s.assign[x]]++] = x;
     }
@@ -531,40 +554,56 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
     if (c->tiles_dirty) {
         rebuild_tiles(c);
         if ((int)c->tiles.size() > c->tile_cap) return fail(SMCCAT_ENOMEM, "tile capacity exceeded");
-        CK(h2d(c, c->d_tiles, c->tiles.data(), c->tiles.size() * sizeof(Tile)));
-        CK(h2d(c, c->d_tile_off, c->tile_off.data(), c->tile_off.size() * sizeof(int32_t)));
-        CK(cudaStreamSynchronize(c->st));  // pageable sources
+        // Pinned staging: the previous tile copy is older than the plan copy
+        // that plan_done (waited on above) tracks, so the buffer is free.
+        std::memcpy(c->h_tiles, c->tiles.data(), c->tiles.size() * sizeof(Tile));
+        std::memcpy(c->h_tile_off, c->tile_off.data(), c->tile_off.size() * sizeof(int32_t));
+        CK(h2d(c, c->d_tiles, c->h_tiles, c->tiles.size() * sizeof(Tile)));
+        CK(h2d(c, c->d_tile_off, c->h_tile_off, c->tile_off.size() * sizeof(int32_t)));
         c->tiles_dirty = false;
     }
 
-    // Pack the plan.
+    // Pack the plan: per-particle job counts, their prefix sums, then every
+    // particle fills its own ranges (in parallel for large batches).
+    struct Cnt { int nn, np, nm, ns; };
+    std::vector<Cnt> cn(count + 1, Cnt{0, 0, 0, 0});
+    // A few microseconds per particle: a small team, since waking a full one
+    // after the previous refresh's GPU wait costs more than it saves.
+    const int team = std::min(kPackThreads, omp_get_max_threads());
+#pragma omp parallel for schedule(static) num_threads(team) if (count >= 2 * kParallelParticles)
+    for (int i = 0; i < count; ++i) {
+        const Slot& s = c->slots[first + i];
+        Cnt x{0, 0, 0, 0};
+        if (on(i)) {
+            const Mirror& m = s.cur;
+            if ((mode == SMCCAT_REFRESH_FULL) || s.full) {
+                x.nn = (int)m.post.size();
+                x.np = N - 1;
+                x.ns = m.K;
+            } else {
+                for (int n : m.post) x.nn += s.dirty_cl[n];
+                for (int n = 0; n < N; ++n) x.np += (s.dirty_p[n] && n != m.root);
+                for (int k = 0; k < m.K; ++k) x.ns += s.dirty_spec[k];
+            }
+            x.nm = m.K * ((x.np + kPmChunk - 1) / kPmChunk);
+        }
+        cn[i + 1] = x;
+    }
+    for (int i = 1; i <= count; ++i) {
+        cn[i].nn += cn[i - 1].nn;
+        cn[i].np += cn[i - 1].np;
+        cn[i].nm += cn[i - 1].nm;
+        cn[i].ns += cn[i - 1].ns;
+    }
+    const int nn = cn[count].nn, np_ = cn[count].np, nm = cn[count].nm, ns = cn[count].ns;
     char* hp = c->h_plan;
     PartHdr* hdr = reinterpret_cast<PartHdr*>(hp);
     size_t off = sizeof(PartHdr) * count;
     NodeJob* nodes = reinterpret_cast<NodeJob*>(hp + off);
-    int nn = 0;
-    for (int i = 0; i < count; ++i) {
-        const Slot& s = c->slots[first + i];
-        if (!on(i)) continue;
-        const bool full = (mode == SMCCAT_REFRESH_FULL) || s.full;
-        if (full) nn += (int)s.cur.post.size();
-        else for (int n : s.cur.post) nn += s.dirty_cl[n];
-    }
     off += sizeof(NodeJob) * nn;
     off = (off + 15) & ~size_t(15);
     PJob* pjobs = reinterpret_cast<PJob*>(hp + off);
     const size_t pjob_off = off;
-    int np_ = 0, nm = 0;
-    for (int i = 0; i < count; ++i) {
-        const Slot& s = c->slots[first + i];
-        if (!on(i)) continue;
-        const bool full = (mode == SMCCAT_REFRESH_FULL) || s.full;
-        int np_i = 0;
-        if (full) np_i = N - 1;
-        else for (int n = 0; n < N; ++n) np_i += (s.dirty_p[n] && n != s.cur.root);
-        np_ += np_i;
-        nm += s.cur.K * ((np_i + kPmChunk - 1) / kPmChunk);
-    }
     off += sizeof(PJob) * np_;
     off = (off + 15) & ~size_t(15);
     PmJob* mjobs = reinterpret_cast<PmJob*>(hp + off);
@@ -573,18 +612,17 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
     off = (off + 15) & ~size_t(15);
     SpecJob* sjobs = reinterpret_cast<SpecJob*>(hp + off);
     const size_t sjob_off = off;
-    int ns = 0;
-    nn = 0;
-    np_ = 0;
-    nm = 0;
+    std::vector<uint8_t> broken(count, 0);
+#pragma omp parallel for schedule(static) num_threads(team) if (count >= 2 * kParallelParticles)
     for (int i = 0; i < count; ++i) {
         const int p = first + i;
         Slot& s = c->slots[p];
         Mirror& m = s.cur;
+        int jn = cn[i].nn, jp = cn[i].np, jm = cn[i].nm, js = cn[i].ns;
         if (!on(i)) {
             PartHdr& h = hdr[i];
             std::memset(&h, 0, sizeof(h));
-            h.node_off = nn;
+            h.node_off = jn;
             continue;
         }
         const bool full = (mode == SMCCAT_REFRESH_FULL) || s.full;
@@ -596,22 +634,22 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
         for (int k = 0; k < m.K; ++k) {
             if (!s.dirty_spec[k]) continue;
             m.sws[k] = 1 - s.old.sws[k];
-            SpecJob& j = sjobs[ns++];
+            SpecJob& j = sjobs[js++];
             j.p = p; j.k = k; j.sws = m.sws[k]; j.pad = 0;
             std::memcpy(j.base, m.base.data(), sizeof(j.base));
             std::memcpy(j.logits, &m.logits[(size_t)k * kStates], sizeof(j.logits));
         }
-        const int pj0 = np_;
+        const int pj0 = jp;
         for (int n = 0; n < N; ++n) {
             if (!s.dirty_p[n] || n == m.root) continue;
             m.pws[n] = 1 - s.old.pws[n];
-            pjobs[np_++] = PJob{p, n, m.pws[n], 0, m.branch[n]};
+            pjobs[jp++] = PJob{p, n, m.pws[n], 0, m.branch[n]};
         }
         for (int k = 0; k < m.K; ++k)
-            for (int q = pj0; q < np_; q += kPmChunk)
-                mjobs[nm++] = PmJob{i, k, q, std::min(kPmChunk, np_ - q)};
+            for (int q = pj0; q < jp; q += kPmChunk)
+                mjobs[jm++] = PmJob{i, k, q, std::min(kPmChunk, jp - q)};
         PartHdr& h = hdr[i];
-        h.node_off = nn;
+        h.node_off = jn;
         for (int n : m.post) {
             if (!s.dirty_cl[n]) continue;
             m.clws[n] = 1 - s.old.clws[n];
@@ -621,11 +659,10 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
             if (c2 >= d.T) ws |= m.clws[c2] << 2;
             ws |= m.pws[c1] << 3;
             ws |= m.pws[c2] << 4;
-            nodes[nn++] = NodeJob{n, c1, c2, ws};
+            nodes[jn++] = NodeJob{n, c1, c2, ws};
         }
-        h.node_cnt = nn - h.node_off;
-        if (h.node_cnt > 0 && nodes[nn - 1].node != m.root)
-            return fail(SMCCAT_EINVAL, "internal error: dirty set does not reach the root");
+        h.node_cnt = jn - h.node_off;
+        if (h.node_cnt > 0 && nodes[jn - 1].node != m.root) broken[i] = 1;
         h.root = m.root;
         h.root_ws = m.clws[m.root];
         h.active = 1;
@@ -640,6 +677,8 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
         s.refreshed = true;
         std::copy(m.sws.begin(), m.sws.end(), c->h_sws + (size_t)p * Kmax);
     }
+    for (int i = 0; i < count; ++i)
+        if (broken[i]) return fail(SMCCAT_EINVAL, "internal error: dirty set does not reach the root");
     const size_t plan_bytes = off + sizeof(SpecJob) * ns;
     CK(h2d(c, c->d_plan, c->h_plan, plan_bytes));
     CK(h2d(c, c->d_sws + (size_t)first * Kmax, c->h_sws + (size_t)first * Kmax, (size_t)count * Kmax));
@@ -697,6 +736,7 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
         CK(cudaEventRecord(c->plan_done, c->st));
         CK(launch(c, SMCCAT_KERNEL_ACCEPT,
                   [&] { return launch_accept(c->d_lnl, c->d_lnl_old, d_mask, first, count, c->st); }));
+#pragma omp parallel for schedule(static) num_threads(team) if (count >= 2 * kParallelParticles)
         for (int i = 0; i < count; ++i) {
             Slot& s = c->slots[first + i];
             if (!on(i) || !s.commit_on_refresh) continue;

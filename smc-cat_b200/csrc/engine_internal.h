@@ -13,6 +13,12 @@
 
 namespace smccat {
 
+// Host loops over at least this many particles (state upload, plan packing,
+// proposals and MH tests) run on OpenMP threads; each iteration touches only
+// its own particle's slot.
+constexpr int kParallelParticles = 32;
+constexpr int kPackThreads = 4;  // threads packing a refresh plan
+
 // Host mirror of one particle's state and of its device workspace indices.
 struct Mirror {
     std::vector<int32_t> parent;   // N
@@ -32,6 +38,7 @@ struct Mirror {
 struct Slot {
     Mirror cur, old;
     std::vector<int32_t> assign;
+    std::vector<int32_t> class_cnt;  // sites per class, kept with `assign`
     std::vector<uint8_t> dirty_cl, dirty_p, dirty_spec;
     bool loaded = false;
     bool full = false;          // next refresh rebuilds everything

@@ -531,16 +531,23 @@ int smccat_rejuvenate(smccat_ctx* c, int32_t first, int32_t count, int32_t itera
     std::vector<double> lnl(count);
     rc = smccat_get_lnl(c, first, count, lnl.data());
     if (rc) return rc;
+#pragma omp parallel for schedule(static) if (count >= kParallelParticles)
     for (int i = 0; i < count; ++i) {
         ps[i].lik = lnl[i] * temperature;
         ps[i].prior = ln_prior(c, first + i, tn);
     }
     std::vector<uint8_t> active(count), mask(count);
+    std::vector<int> prc(count);
+    std::vector<std::string> perr(count);
+    std::vector<double> nprior(count);
     for (;;) {
-        int n_active = 0;
+        // Proposals on the host mirrors; each particle has its own generator
+        // and touches only its own slot, so they run in parallel.
+#pragma omp parallel for schedule(dynamic, 8) if (count >= kParallelParticles)
         for (int i = 0; i < count; ++i) {
             PS& q = ps[i];
             active[i] = 0;
+            prc[i] = SMCCAT_OK;
             while (!q.done && q.left == 0) {
                 if (q.iter == iterations) { q.done = true; break; }
                 const double u = unif(q.g);  // Mcmc.cpp:40-50
@@ -551,11 +558,19 @@ int smccat_rejuvenate(smccat_ctx* c, int32_t first, int32_t count, int32_t itera
                 q.iter++;
             }
             if (q.done) continue;
-            rc = propose(c, first + i, q.family, q.g, tn, &q.pr);
-            if (rc) return rc;
+            const int r = propose(c, first + i, q.family, q.g, tn, &q.pr);
+            if (r) {
+                prc[i] = r;
+                perr[i] = smccat_last_error();  // the message is per thread
+                continue;
+            }
             q.left--;
             active[i] = 1;
-            ++n_active;
+        }
+        int n_active = 0;
+        for (int i = 0; i < count; ++i) {
+            if (prc[i]) return mfail(prc[i], perr[i]);
+            n_active += active[i];
         }
         if (n_active == 0) break;
         rc = refresh_internal(c, first, count, SMCCAT_REFRESH_DIRTY, active.data());
@@ -563,19 +578,21 @@ int smccat_rejuvenate(smccat_ctx* c, int32_t first, int32_t count, int32_t itera
         rc = smccat_get_lnl(c, first, count, lnl.data());
         if (rc) return rc;
         st.lockstep_steps++;
+#pragma omp parallel for schedule(static) if (count >= kParallelParticles)
+        for (int i = 0; i < count; ++i)
+            if (active[i]) nprior[i] = ln_prior(c, first + i, tn);
         for (int i = 0; i < count; ++i) {
             mask[i] = 1;
             if (!active[i]) continue;
             PS& q = ps[i];
-            const double nprior = ln_prior(c, first + i, tn);
             const double nlik = lnl[i] * temperature;
-            const double ratio = (nprior + nlik) - (q.prior + q.lik) + q.pr.hastings;  // Mcmc.cpp:57-60
+            const double ratio = (nprior[i] + nlik) - (q.prior + q.lik) + q.pr.hastings;  // Mcmc.cpp:57-60
             const bool ok = std::log(unif(q.g)) <= ratio;
             mask[i] = ok ? 1 : 0;
             st.proposed[q.pr.kind]++;
             if (ok) {
                 st.accepted[q.pr.kind]++;
-                q.prior = nprior;
+                q.prior = nprior[i];
                 q.lik = nlik;
             }
         }
