@@ -12,12 +12,12 @@
 //                 stages its two children's P blocks into shared memory with TMA
 //                 bulk copies (double-buffered, mbarrier-tracked, the next node's
 //                 copy in flight while the current node computes), keeps the
-//                 partial it just produced in
-//                 registers (in a post-order of an upward-closed dirty set the
-//                 previous node is always a child of the next one), reads at most
-//                 one child partial back from memory, rescales each (site, rate)
-//                 by an exact power of two, then the CTA reduces the root
-//                 (Particle.cpp:634-674): log-sum-exp over rates, +I, warp sum.
+//                 partial it just produced in registers (in a post-order of an
+//                 upward-closed dirty set the previous node is always a child of
+//                 the next one), reads at most one child partial back from
+//                 memory, rescales each (site, rate) by an exact power of two,
+//                 then the CTA reduces the root (Particle.cpp:634-674):
+//                 log-sum-exp over rates, +I, warp sum.
 //   reduce_kernel per particle, sums the tile partials in a fixed order.
 #include <cuda_runtime.h>
 #include <math.h>
@@ -273,7 +273,6 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
 
     extern __shared__ __align__(128) unsigned char smem_raw[];  // [R warps][2 buffers][2 children][kPBlock]
     __shared__ __align__(8) uint64_t bars[R][2];
-    __shared__ double red[R][32 * W];
     __shared__ int bad;
 
     const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
@@ -290,6 +289,13 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
         col[w] = r * d.Spad + slot;
     }
     T* buf = reinterpret_cast<T*>(smem_raw) + (size_t)r * 4 * kPBlock;
+    // Root-reduction row of warp rr: the start of that warp's own P buffers,
+    // free once the warp has left its node loop (every copy into them has been
+    // waited on). Keeping it out of static shared memory lets four CTAs share
+    // an SM.
+    auto red = [&](int rr) {
+        return reinterpret_cast<double*>(smem_raw + (size_t)rr * 4 * kPBlock * sizeof(T));
+    };
 
     const size_t j_stride = (size_t)R * d.Spad;
     const size_t ws_stride = (size_t)kStates * j_stride;
@@ -459,6 +465,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
         }
         bad = 1;
     }
+    __syncwarp();  // the warp's buffers are free from here on (red(r) reuses them)
     // Root reduction for this tile.
     if (cnt == 0 && valid) {
         const T* xp = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride;
@@ -479,7 +486,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
             double s = 0.0;
 #pragma unroll
             for (int i = 0; i < kStates; ++i) s = fma(pi[i], (double)y[w][i], s);
-            red[r][lane + 32 * w] = log(s) + lsc[w];
+            red(r)[lane + 32 * w] = log(s) + lsc[w];
         }
     }
     __syncthreads();
@@ -489,14 +496,14 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
         for (int w = 0; w < W; ++w) {
             if (!vw[w]) continue;
             const int q = lane + 32 * w;
-            double mx = red[0][q];
+            double mx = red(0)[q];
 #pragma unroll
-            for (int rr = 1; rr < R; ++rr) mx = fmax(mx, red[rr][q]);
+            for (int rr = 1; rr < R; ++rr) mx = fmax(mx, red(rr)[q]);
             double lse = mx;
             if (mx > -INFINITY) {
                 double se = 0.0;
 #pragma unroll
-                for (int rr = 0; rr < R; ++rr) se += exp(red[rr][q] - mx);
+                for (int rr = 0; rr < R; ++rr) se += exp(red(rr)[q] - mx);
                 lse = mx + log(se);
             }
             // +I mixing, Particle.cpp:667-670, evaluated in log space.
@@ -574,11 +581,12 @@ cudaError_t launch_prune_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
 
 // SIMT variants as (sites per lane W, CTAs per SM MINB, mat-vec rows in flight RB):
 //   R = 4:  0 (1,4,1)  1 (1,3,1)  2 (1,2,1)  3 (1,3,4)  4 (1,4,4)  5 (1,2,4)  6 (2,2,1)
+//           7 (1,4,2)  8 (1,3,2)
 //           FP32 only, where 40 registers hold a lane's two 20-vectors:
-//           7 (1,5,1)  8 (1,6,1)  9 (1,5,4)
+//           9 (1,5,1)  10 (1,6,1)  11 (1,5,4)
 //   other:  0 (1,-,1)  1 (1,-,4)  2 (2,-,1)
 // W = 2 variants take 64-slot tiles, the others 32-slot tiles.
-int simt_variants(int R, bool fp32) { return R == 4 ? (fp32 ? 10 : 7) : 3; }
+int simt_variants(int R, bool fp32) { return R == 4 ? (fp32 ? 12 : 9) : 3; }
 int simt_width(int R, int v) { return (R == 4 ? v == 6 : v == 2) ? 2 : 1; }
 
 template <class T, int R, int MINB, int MINB2>
@@ -599,6 +607,8 @@ cudaError_t launch_prune_r4(const PruneArgs& a, int ntiles, int variant, cudaStr
         case 4: return launch_prune_t<T, 4, 4, 1, 4>(a, ntiles, st);
         case 5: return launch_prune_t<T, 4, 2, 1, 4>(a, ntiles, st);
         case 6: return launch_prune_t<T, 4, 2, 2, 1>(a, ntiles, st);
+        case 7: return launch_prune_t<T, 4, 4, 1, 2>(a, ntiles, st);
+        case 8: return launch_prune_t<T, 4, 3, 1, 2>(a, ntiles, st);
         default: return launch_prune_t<T, 4, 4, 1, 1>(a, ntiles, st);
     }
 }
@@ -621,9 +631,9 @@ cudaError_t launch_prune_typed(const PruneArgs& a, int ntiles, int variant, cuda
 cudaError_t launch_prune_fp32(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
     if (a.d.R == 4) {
         switch (variant) {
-            case 7: return launch_prune_t<float, 4, 5, 1, 1>(a, ntiles, st);
-            case 8: return launch_prune_t<float, 4, 6, 1, 1>(a, ntiles, st);
-            case 9: return launch_prune_t<float, 4, 5, 1, 4>(a, ntiles, st);
+            case 9: return launch_prune_t<float, 4, 5, 1, 1>(a, ntiles, st);
+            case 10: return launch_prune_t<float, 4, 6, 1, 1>(a, ntiles, st);
+            case 11: return launch_prune_t<float, 4, 5, 1, 4>(a, ntiles, st);
             default: break;
         }
     }
