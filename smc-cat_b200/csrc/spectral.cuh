@@ -101,35 +101,35 @@ static __device__ __noinline__ void spectral_decompose_warp_ws(const double* __r
                 const double apq = A[p][q];
                 double c = 1.0, s = 0.0;
                 if (apq != 0.0) {
-                    const double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
-                    double t = 1.0 / (fabs(theta) + sqrt(theta * theta + 1.0));
-                    if (theta < 0.0) t = -t;
-                    c = 1.0 / sqrt(t * t + 1.0);
+                    // t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)), theta =
+                    // (A_qq - A_pp) / (2 A_pq), written with one division.
+                    const double dd = A[q][q] - A[p][p];
+                    double t = 2.0 * apq / (fabs(dd) + sqrt(dd * dd + 4.0 * apq * apq));
+                    if (dd < 0.0) t = -t;
+                    c = rsqrt(t * t + 1.0);
                     s = t * c;
                 }
                 pp[lane] = p; qq[lane] = q; cs[lane] = c; sn[lane] = s;
             }
             __syncwarp();
-            for (int idx = lane; idx < 10 * kStates; idx += 32) {  // columns
-                const int m = idx / kStates, k = idx % kStates;
-                const int p = pp[m], q = qq[m];
-                const double c = cs[m], s = sn[m];
-                const double akp = A[k][p], akq = A[k][q];
-                A[k][p] = c * akp - s * akq;
-                A[k][q] = s * akp + c * akq;
+            // A <- G^T A G block by block: the 10 pairs partition the indices, so
+            // each 2 x 2 block (pair m1 rows, pair m2 columns) belongs to one lane.
+            // Columns rotate by pair m2, then rows by pair m1; a rotated pair's
+            // own off-diagonal entry is set to zero.
+            for (int idx = lane; idx < 100; idx += 32) {
+                const int m1 = idx / 10, m2 = idx % 10;
+                const int p1 = pp[m1], q1 = qq[m1], p2 = pp[m2], q2 = qq[m2];
+                const double c1 = cs[m1], s1 = sn[m1], c2 = cs[m2], s2 = sn[m2];
+                const double a_pp = A[p1][p2], a_pq = A[p1][q2], a_qp = A[q1][p2], a_qq = A[q1][q2];
+                const double b_pp = c2 * a_pp - s2 * a_pq, b_pq = s2 * a_pp + c2 * a_pq;
+                const double b_qp = c2 * a_qp - s2 * a_qq, b_qq = s2 * a_qp + c2 * a_qq;
+                const bool zero = m1 == m2 && s1 != 0.0;
+                A[p1][p2] = c1 * b_pp - s1 * b_qp;
+                A[q1][q2] = s1 * b_pq + c1 * b_qq;
+                A[p1][q2] = zero ? 0.0 : c1 * b_pq - s1 * b_qq;
+                A[q1][p2] = zero ? 0.0 : s1 * b_pp + c1 * b_qp;
             }
-            __syncwarp();
-            for (int idx = lane; idx < 10 * kStates; idx += 32) {  // rows
-                const int m = idx / kStates, k = idx % kStates;
-                const int p = pp[m], q = qq[m];
-                const double c = cs[m], s = sn[m];
-                const double apk = A[p][k], aqk = A[q][k];
-                A[p][k] = c * apk - s * aqk;
-                A[q][k] = s * apk + c * aqk;
-            }
-            __syncwarp();
-            if (lane < 10 && sn[lane] != 0.0) { A[pp[lane]][qq[lane]] = 0.0; A[qq[lane]][pp[lane]] = 0.0; }
-            for (int idx = lane; idx < 10 * kStates; idx += 32) {  // eigenvectors
+            for (int idx = lane; idx < 10 * kStates; idx += 32) {  // eigenvectors, V <- V G
                 const int m = idx / kStates, k = idx % kStates;
                 const int p = pp[m], q = qq[m];
                 const double c = cs[m], s = sn[m];
