@@ -66,6 +66,9 @@ def parse():
                     help="comma-separated CAT configs (e.g. 3,4) to time in particle waves")
     ap.add_argument("--extra-particles", type=int, default=0,
                     help="particles for --extra-configs (default: the configuration's)")
+    ap.add_argument("--gibbs-particles", type=int, default=32,
+                    help="particles of a CAT --extra-configs run timed through one Gibbs pass "
+                         "and one learned-proposal pass (0 to skip)")
     return ap.parse_args()
 
 
@@ -197,7 +200,45 @@ def cpu_baseline(cfg, codes, st, n_sample, min_seconds=10.0):
                       f"{reps} repetitions in {el:.1f} s (FP64 oracle, OpenMP over particles)"}
 
 
-def measure_config_waves(cid, steps, local, rank, particles=0, oracle_sample=2):
+def measure_reassignment(codes, st, cfg, n, local, torch):
+    """One Gibbs pass (Neal 8, floor(S/2) site iterations per particle, then
+    the re-permutation and full refresh) and one learned-proposal pass of the
+    same length on the first n particles, wall-clocked around
+    device-synchronised calls; the MLP is trained first (untimed). The context
+    has 32 class slots beyond the particles' largest K, since Gibbs opens new
+    classes."""
+    import smccat
+    kmax = st["logits"].shape[1] + 32
+    logits = np.zeros((n, kmax, 20))
+    logits[:, :st["logits"].shape[1]] = st["logits"][:n]
+    eng = smccat.Engine(codes, cfg.R, n, max_classes=kmax, lg=cfg.lg, invar=cfg.invar,
+                        cat=cfg.cat, device=local)
+    eng.set_particles(0, st["parent"][:n], st["branch"][:n], st["base"][:n],
+                      st["num_classes"][:n], logits, st["assign"][:n], st["pinv"][:n],
+                      st["shape"][:n])
+    eng.refresh(full=True)
+    its = cfg.S // 2
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    gs = eng.gibbs(temperature=1.0, seed=11, first=0, count=n)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    loss = eng.learned_train(epochs=1, batch_sites=512, lr=1e-3, seed=3, first=0, count=min(n, 8))
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    ls = eng.learned_move(updates=its, temperature=1.0, seed=12, first=0, count=n)
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    eng.close()
+    return {"particles": n, "site_iterations_per_particle": its,
+            "gibbs": {"seconds": t1 - t0, "site_iterations_per_s": n * its / (t1 - t0),
+                      "classes_before": gs["classes_before"], "classes_after": gs["classes_after"]},
+            "learned": {"train_seconds": t2 - t1, "train_loss": loss, "seconds": t3 - t2,
+                        "site_updates_per_s": n * its / (t3 - t2),
+                        "acceptance": ls["accepted"] / max(ls["proposed"], 1)}}
+
+
+def measure_config_waves(cid, steps, local, rank, particles=0, oracle_sample=2, gibbs_particles=0):
     """Full-refresh throughput of a configuration whose particles may not fit
     one context: particles stream through the device in waves (upload states,
     refreshLikelihood(true), read log-likelihoods), at FP64 and at FP32; the
@@ -259,6 +300,9 @@ def measure_config_waves(cid, steps, local, rank, particles=0, oracle_sample=2):
                      "kernel_ms_per_pass": {k: round(v, 3) for k, v in prof["ms"].items()},
                      "prune_variant": eng.kernel_variants()[1]}
         eng.close()
+        if cfg.cat and name == "fp64" and gibbs_particles > 0:
+            res["reassignment"] = measure_reassignment(codes, st, cfg, min(gibbs_particles, n),
+                                                       local, torch)
     d = np.abs(lnls["fp32"] - lnls["fp64"])
     res["fp32_vs_fp64_abs_dlogl"] = {"max": float(d.max()), "mean": float(d.mean())}
     o = []
@@ -535,7 +579,8 @@ def main():
         if args.extra_configs:
             line["extra_configs"] = [
                 measure_config_waves(int(c), max(1, args.steps // 5), local, rank,
-                                     particles=args.extra_particles)
+                                     particles=args.extra_particles,
+                                     gibbs_particles=args.gibbs_particles)
                 for c in args.extra_configs.split(",") if c.strip()]
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(cfg, codes, st, args.cpu_sample)

@@ -240,6 +240,20 @@ int smccat_set_rate_cholesky(smccat_ctx* ctx, const double* lower190x190);
 int smccat_set_split_posteriors(smccat_ctx* ctx, int32_t n, const uint64_t* bits,
                                 const double* prob);
 
+/* computeSplitPosteriors (Miscellaneous.hpp:115-150) over the trees of
+ * particles [first, first+count): each particle contributes its clade set
+ * (Tree::getSplitSet, Tree.cpp:485-541: the taxon set of every non-root node,
+ * canonicalised so that taxon 0 is set, each distinct set once) with weight
+ * weights[i], or 1/count when weights is NULL (the resampled-assignment form,
+ * Miscellaneous.hpp:135-150). The result replaces the split posteriors the
+ * adaptive NNI move reads, as smccat_set_split_posteriors would. *n_out gets
+ * the number of distinct splits; if bits and prob are not NULL, the first
+ * min(n, cap) of them are written in the layout of smccat_set_split_posteriors,
+ * by decreasing probability (ties by bits). At most 128 taxa. */
+int smccat_compute_split_posteriors(smccat_ctx* ctx, int32_t first, int32_t count,
+                                    const double* weights, int32_t cap, int32_t* n_out,
+                                    uint64_t* bits, double* prob);
+
 /* Particle::lnPrior (Particle.cpp:484-517) of the current states. */
 int smccat_ln_prior(smccat_ctx* ctx, int32_t first, int32_t count, double* out);
 

@@ -455,6 +455,49 @@ int smccat_set_split_posteriors(smccat_ctx* c, int32_t n, const uint64_t* bits, 
     return SMCCAT_OK;
 }
 
+int smccat_compute_split_posteriors(smccat_ctx* c, int32_t first, int32_t count,
+                                    const double* weights, int32_t cap, int32_t* n_out,
+                                    uint64_t* bits, double* prob) {
+    if (!c || !n_out) return mfail(SMCCAT_EINVAL, "null argument");
+    const Dims& d = dims_of(c);
+    if (d.T > 128) return mfail(SMCCAT_EINVAL, "split bit sets hold at most 128 taxa");
+    if (first < 0 || count < 1 || cap < 0) return mfail(SMCCAT_EINVAL, "bad range");
+    for (int i = 0; i < count; ++i)
+        if (!slot_of(c, first + i).loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
+    auto less = [](const Split& a, const Split& b) {
+        return a.w[1] != b.w[1] ? a.w[1] < b.w[1] : a.w[0] < b.w[0];
+    };
+    std::unordered_map<Split, double, SplitHash> acc;
+    for (int i = 0; i < count; ++i) {  // particle order fixes the summation order
+        WTree t;
+        t.load(slot_of(c, first + i).cur, d.T);
+        const std::vector<Split> sp = t.splits();
+        std::vector<Split> set;
+        set.reserve(sp.size());
+        for (int n = 0; n < t.N; ++n)
+            if (n != t.root) set.push_back(sp[n]);
+        std::sort(set.begin(), set.end(), less);
+        set.erase(std::unique(set.begin(), set.end()), set.end());
+        const double w = weights ? weights[i] : 1.0 / count;
+        for (const Split& x : set) acc[x] += w;
+    }
+    tuning_of(c).split_post = acc;
+    *n_out = (int32_t)acc.size();
+    if (bits && prob) {
+        std::vector<std::pair<Split, double>> v(acc.begin(), acc.end());
+        std::sort(v.begin(), v.end(), [&](const auto& a, const auto& b) {
+            return a.second != b.second ? a.second > b.second : less(a.first, b.first);
+        });
+        const int m = std::min<int>(cap, (int)v.size());
+        for (int i = 0; i < m; ++i) {
+            bits[2 * i] = v[i].first.w[0];
+            bits[2 * i + 1] = v[i].first.w[1];
+            prob[i] = v[i].second;
+        }
+    }
+    return SMCCAT_OK;
+}
+
 int smccat_ln_prior(smccat_ctx* c, int32_t first, int32_t count, double* out) {
     if (!c || !out) return mfail(SMCCAT_EINVAL, "null argument");
     const Tuning& tn = tuning_of(c);

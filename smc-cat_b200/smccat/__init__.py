@@ -130,6 +130,8 @@ def lib():
         "smccat_set_rate_cholesky": ([vp, _dp], ctypes.c_int),
         "smccat_set_split_posteriors": ([vp, _i32, ctypes.POINTER(ctypes.c_uint64), _dp],
                                         ctypes.c_int),
+        "smccat_compute_split_posteriors": ([vp, _i32, _i32, _dp, _i32, _ip,
+                                             ctypes.POINTER(ctypes.c_uint64), _dp], ctypes.c_int),
         "smccat_ln_prior": ([vp, _i32, _i32, _dp], ctypes.c_int),
         "smccat_propose": ([vp, _i32, _i32, ctypes.c_uint64, _ip, _dp], ctypes.c_int),
         "smccat_rejuvenate": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64,
@@ -341,6 +343,25 @@ class Engine:
         pr, prp = _d(probs)
         _check(lib().smccat_set_split_posteriors(
             self._h, len(pr), b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), prp))
+
+    def compute_split_posteriors(self, weights=None, first=0, count=None, cap=None):
+        """computeSplitPosteriors over the particles' trees; also installs the
+        result for the adaptive NNI move. Returns (bits [n, 2] uint64, prob [n])."""
+        count = self.P - first if count is None else count
+        wp = None
+        if weights is not None:
+            w, wp = _d(weights)
+        n = ctypes.c_int32(0)
+        _check(lib().smccat_compute_split_posteriors(self._h, int(first), int(count), wp, 0,
+                                                     ctypes.byref(n), None, None))
+        cap = n.value if cap is None else int(cap)
+        bits = np.zeros((max(cap, 1), 2), dtype=np.uint64)
+        prob = np.zeros(max(cap, 1))
+        _check(lib().smccat_compute_split_posteriors(
+            self._h, int(first), int(count), wp, cap, ctypes.byref(n),
+            bits.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), prob.ctypes.data_as(_dp)))
+        m = min(cap, n.value)
+        return bits[:m], prob[:m]
 
     def ln_prior(self, first=0, count=None) -> np.ndarray:
         count = self.P - first if count is None else count

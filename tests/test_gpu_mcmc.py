@@ -318,3 +318,44 @@ def test_gibbs_at_zero_temperature_samples_the_crp_prior():
     expected = sum(alpha / (alpha + i) for i in range(cfg.S))
     assert abs(np.mean(ks) - expected) < 0.1 * expected, (np.mean(ks), expected)
     eng.close()
+
+
+def test_split_posteriors_match_oracle_and_drive_adaptive_nni():
+    """computeSplitPosteriors (Miscellaneous.hpp:115-150) over the particles'
+    clade sets (Tree.cpp:485-541), uniform and weighted, against the oracle;
+    the result then sets the adaptive NNI node weights."""
+    from oracle import splits
+    eng, codes, st = engine()
+    T = CFG.T
+    w = np.random.default_rng(4).random(CFG.particles)
+    w /= w.sum()
+    for weights in (w, None):
+        bits, prob = eng.compute_split_posteriors(weights)
+        ref = splits.split_posteriors(st["parent"], T, weights)
+        got = {(int(b[0]), int(b[1])): float(p) for b, p in zip(bits, prob)}
+        assert set(got) == set(ref)
+        for k, v in ref.items():
+            assert got[k] == pytest.approx(v, rel=1e-14, abs=1e-15)
+        assert np.all(np.diff(prob) <= 0)
+    # The uniform table is now installed: adaptive NNI proposals must carry the
+    # Hastings ratio of node weights built from it.
+    post = {frozenset(t for t in range(T) if (k[t >> 6] >> (t & 63)) & 1): v for k, v in ref.items()}
+    seen = 0
+    for seed in range(60):
+        p = seed % CFG.particles
+        before = eng.get_particles()["parent"][p]
+        kind, h = eng.propose(p, smccat.FAMILY_TREE, 5000 + seed)
+        after = eng.get_particles()["parent"][p]
+        if kind == smccat.MOVE_NAMES.index("Adaptive NNI"):
+            seen += 1
+            u, v = np.where(before != after)[0]
+            cand = {int(before[u]), int(before[v])}
+            x = [c for c in cand if int(before[c]) in cand][0]
+            w0 = _weights(before, T, post)
+            w1 = _weights(after, T, post)
+            ref_h = np.log(w1[x] / sum(w1.values())) - np.log(w0[x] / sum(w0.values()))
+            assert h == pytest.approx(ref_h, rel=1e-10, abs=1e-12)
+        eng.refresh()
+        eng.accept(np.zeros(CFG.particles, np.uint8))
+    assert seen >= 5
+    eng.close()

@@ -163,3 +163,17 @@ def test_all_gap_site_is_zero_without_invariants():
                          0.0, [0.5, 1.5], site_out=True)
     # log(sum_r exp(0)) = log R: the reference has no 1/R weight
     np.testing.assert_allclose(site, np.log(2.0), atol=1e-13)
+
+
+def test_split_set_known_answer():
+    """((0,1),(2,3)) rooted at node 6: tips and both cherries; the root's two
+    children give the same canonical split, counted once (Tree.cpp:485-541)."""
+    from oracle import splits
+    parent = [4, 4, 5, 5, 6, 6, -1]
+    got = splits.split_set(parent, 4)
+    want = {0b0001, 0b1101, 0b1011, 0b0111, 0b0011}
+    assert got == {(b, 0) for b in want}
+    post = splits.split_posteriors([parent, parent, [4, 5, 4, 5, 6, 6, -1]], 4)
+    assert post[(0b0011, 0)] == pytest.approx(2 / 3)
+    assert post[(0b0101, 0)] == pytest.approx(1 / 3)
+    assert post[(0b0001, 0)] == pytest.approx(1.0)
