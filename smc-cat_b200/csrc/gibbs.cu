@@ -53,12 +53,29 @@ __device__ void fill_exp(const GibbsArgs& a, int i, int k, const double* rec, do
     }
 }
 
-// Log-likelihood of site s under class slot k and rate r, one warp.
-__device__ double site_rate_lnl(const GibbsArgs& a, int i, int s, int r, const double* rec,
-                                const double* ex, double* stash) {
+// Rates per warp in the Gibbs weights (all of a class's rates together) and in
+// the learned move (which spreads its two classes' rates over more warps).
+constexpr int kRateBlock = 4;
+constexpr int kRateBlockLearned = 2;
+
+// Log-likelihoods of one site under one class for rates [r0, r0 + RB) (those
+// below R), one warp: lanes are states and the rate chains interleave.
+// Single-site pruning in the eigenbasis, P(t r) x = L (exp(lambda t r) o (Rm x)).
+// The vectors every lane needs whole (x before Rm, z before L) pass through the
+// warp's shared exchange row `xch` [RB][kStates] and are read back as broadcast
+// pairs, not shuffled lane by lane. The node computed last stays in registers
+// (in post-order it is a child of the next node); other internal children come
+// back from the warp's stash [NI][RB][32]. Tip codes of the site come from
+// `scode` (shared). out[b] = log L of rate r0 + b.
+template <int RB>
+__device__ void site_class_lnl(const GibbsArgs& a, int i, int r0, const double* rec,
+                               const double* ex, double* stash, const uint8_t* scode,
+                               double* xch, double* out) {
+    using D2 = double2;
     const Dims& d = a.d;
     const int lane = threadIdx.x & 31;
     const int li = lane < kStates ? lane : 0;
+    const bool st_lane = lane < kStates;
     double Lrow[kStates], Rrow[kStates];
 #pragma unroll
     for (int m = 0; m < kStates; ++m) {
@@ -68,52 +85,105 @@ __device__ double site_rate_lnl(const GibbsArgs& a, int i, int s, int r, const d
     double rs = 0.0;
 #pragma unroll
     for (int j = 0; j < kStates; ++j) rs += Rrow[j];
+    bool on[RB];
+    double v[RB], lsc[RB];
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+        on[b] = r0 + b < d.R;
+        v[b] = 1.0;
+        lsc[b] = 0.0;
+    }
     const int32_t* tree = a.tree + (size_t)i * d.NI * 3;
-    double lsc = 0.0, v = 1.0;
+    int prev = -1;
     for (int q = 0; q < d.NI; ++q) {
         const int n = tree[3 * q];
-        v = 1.0;
+        double vn[RB];
+#pragma unroll
+        for (int b = 0; b < RB; ++b) vn[b] = 1.0;
 #pragma unroll 1
         for (int ci = 1; ci <= 2; ++ci) {
             const int c = tree[3 * q + ci];
-            const double e = ex[((size_t)c * d.R + r) * kStates + li];
-            double z;  // lane m: exp(lambda_m t) * (Rm x)_m
+            double e[RB], z[RB];
+#pragma unroll
+            for (int b = 0; b < RB; ++b)
+                e[b] = on[b] ? ex[((size_t)c * d.R + r0 + b) * kStates + li] : 0.0;
             if (c < d.T) {
-                const int code = a.codes[(size_t)c * d.S + s];
+                const int code = scode[c];
                 double rc = rs;
                 if (code < kStates) {
 #pragma unroll
                     for (int j = 0; j < kStates; ++j) rc = (j == code) ? Rrow[j] : rc;
                 }
-                z = e * rc;
+#pragma unroll
+                for (int b = 0; b < RB; ++b) z[b] = e[b] * rc;
             } else {
-                const double xv = stash[(size_t)(c - d.T) * 32 + lane];
-                double acc = 0.0;
 #pragma unroll
-                for (int j = 0; j < kStates; ++j) acc = fma(Rrow[j], __shfl_sync(0xffffffffu, xv, j), acc);
-                z = e * acc;
+                for (int b = 0; b < RB; ++b) {
+                    const double xv = (c == prev) ? v[b]
+                                                  : stash[((size_t)(c - d.T) * RB + b) * 32 + lane];
+                    if (st_lane) xch[b * kStates + lane] = xv;
+                }
+                __syncwarp();
+                double acc[RB];
+#pragma unroll
+                for (int b = 0; b < RB; ++b) acc[b] = 0.0;
+#pragma unroll
+                for (int j = 0; j < kStates / 2; ++j) {
+#pragma unroll
+                    for (int b = 0; b < RB; ++b) {
+                        const D2 x2 = reinterpret_cast<const D2*>(xch + b * kStates)[j];
+                        acc[b] = fma(Rrow[2 * j], x2.x, acc[b]);
+                        acc[b] = fma(Rrow[2 * j + 1], x2.y, acc[b]);
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int b = 0; b < RB; ++b) z[b] = e[b] * acc[b];
             }
-            double y = 0.0;
 #pragma unroll
-            for (int m = 0; m < kStates; ++m) y = fma(Lrow[m], __shfl_sync(0xffffffffu, z, m), y);
-            v *= y;
+            for (int b = 0; b < RB; ++b)
+                if (st_lane) xch[b * kStates + lane] = z[b];
+            __syncwarp();
+            double y[RB];
+#pragma unroll
+            for (int b = 0; b < RB; ++b) y[b] = 0.0;
+#pragma unroll
+            for (int m = 0; m < kStates / 2; ++m) {
+#pragma unroll
+                for (int b = 0; b < RB; ++b) {
+                    const D2 z2 = reinterpret_cast<const D2*>(xch + b * kStates)[m];
+                    y[b] = fma(Lrow[2 * m], z2.x, y[b]);
+                    y[b] = fma(Lrow[2 * m + 1], z2.y, y[b]);
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int b = 0; b < RB; ++b) vn[b] *= y[b];
         }
-        if (lane >= kStates) v = 0.0;
-        const double mx = warp_max20(v);
-        if (mx > 0.0) {
-            int e;
-            frexp(mx, &e);
-            v *= ldexp(1.0, -e);
-            lsc += e * 0.69314718055994530942;
-        } else {
-            lsc = -INFINITY;
+#pragma unroll
+        for (int b = 0; b < RB; ++b) {
+            double x = st_lane ? vn[b] : 0.0;
+            const double mx = warp_max20(x);
+            if (mx > 0.0) {
+                int e;
+                frexp(mx, &e);
+                x *= ldexp(1.0, -e);
+                lsc[b] += e * 0.69314718055994530942;
+            } else {
+                lsc[b] = -INFINITY;
+            }
+            v[b] = x;
+            stash[((size_t)(n - d.T) * RB + b) * 32 + lane] = x;
         }
-        stash[(size_t)(n - d.T) * 32 + lane] = v;
+        prev = n;
         __syncwarp();
     }
-    const double pi = (lane < kStates) ? rec[kSpecPi + lane] : 0.0;
-    const double sv = wsum(pi * v);
-    return log(sv) + lsc;
+    const double pi = st_lane ? rec[kSpecPi + lane] : 0.0;
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+        const double sv = wsum(pi * v[b]);
+        if (lane == 0 && on[b]) out[b] = log(sv) + lsc[b];
+    }
 }
 
 __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
@@ -124,13 +194,15 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
     const int Kcap = a.Kcap;
     double* spec = a.spec + (size_t)i * (Kcap + kAux) * kSpecStride;
     double* ex = a.expt + (size_t)i * (Kcap + kAux) * d.N * d.R * kStates;
-    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * d.NI * 32;
+    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * d.NI * kRateBlock * 32;
+    __shared__ __align__(16) double xch[kGibbsWarps][kRateBlock * kStates];
     double* logits = a.logits + (size_t)i * (Kcap + kAux) * kStates;
     int32_t* assign = a.assign + (size_t)i * d.S;
     const double* base = a.base + (size_t)i * kBase;
     extern __shared__ double sh[];                   // lnl [(Kcap + kAux) * R]
     double* wts = sh + (size_t)(Kcap + kAux) * d.R;  // [Kcap + kAux]
     int* counts = reinterpret_cast<int*>(wts + (Kcap + kAux));  // [Kcap + kAux]
+    uint8_t* scode = reinterpret_cast<uint8_t*>(counts + (Kcap + kAux));  // [T]: the site's column
     const bool weights_mode = gp.fixed_site >= 0;
     __shared__ int s_site, s_kcur, s_choice;
     __shared__ SpecWork work[kAux];
@@ -174,6 +246,7 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
         }
         __syncthreads();
         const int s = s_site, kcur = s_kcur;
+        for (int c = threadIdx.x; c < d.T; c += blockDim.x) scode[c] = a.codes[(size_t)c * d.S + s];
         // 2. diagonalise the auxiliary classes (Particle.cpp:823-833)
         if (warp < kAux)
             spectral_decompose_warp_ws(base, logits + (size_t)(kcur + warp) * kStates,
@@ -183,15 +256,17 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
             fill_exp(a, i, kcur + j, spec + (size_t)(kcur + j) * kSpecStride,
                      ex + (size_t)(kcur + j) * d.N * d.R * kStates);
         __syncthreads();
-        // 3. site log-likelihood per (class, rate) (Particle.cpp:857-930)
-        const int npairs = (kcur + kAux) * d.R;
-        for (int pr = warp; pr < npairs; pr += kGibbsWarps) {
-            const int k = pr / d.R, r = pr % d.R;
-            double l = -INFINITY;
-            if (k >= kcur || counts[k] > 0)
-                l = site_rate_lnl(a, i, s, r, spec + (size_t)k * kSpecStride,
-                                  ex + (size_t)k * d.N * d.R * kStates, stash);
-            if (lane == 0) sh[pr] = l;
+        // 3. site log-likelihood per (class, rate) (Particle.cpp:857-930): one
+        // warp per class, all its rates together
+        for (int k = warp; k < kcur + kAux; k += kGibbsWarps) {
+            if (k >= kcur || counts[k] > 0) {
+                for (int r0 = 0; r0 < d.R; r0 += kRateBlock)
+                    site_class_lnl<kRateBlock>(a, i, r0, spec + (size_t)k * kSpecStride,
+                                               ex + (size_t)k * d.N * d.R * kStates, stash, scode,
+                                               xch[warp], sh + (size_t)k * d.R + r0);
+            } else if (lane == 0) {
+                for (int r = 0; r < d.R; ++r) sh[(size_t)k * d.R + r] = -INFINITY;
+            }
         }
         __syncthreads();
         // 4. weights and the draw (Particle.cpp:931-978)
@@ -354,7 +429,8 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
     const int K = gp.K;
     double* spec = a.spec + (size_t)i * (a.Kcap + kAux) * kSpecStride;
     double* ex = a.expt + (size_t)i * (a.Kcap + kAux) * d.N * d.R * kStates;
-    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * d.NI * 32;
+    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * d.NI * kRateBlockLearned * 32;
+    __shared__ __align__(16) double xch[kGibbsWarps][kRateBlockLearned * kStates];
     const double* logits = a.logits + (size_t)i * (a.Kcap + kAux) * kStates;
     int32_t* assign = a.assign + (size_t)i * d.S;
     const double* base = a.base + (size_t)i * kBase;
@@ -364,6 +440,7 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
     float* hs = xs + kGibbsWarps * kMlpIn;                                   // [warps][kMlpHid]
     float* score = hs + kGibbsWarps * kMlpHid;                               // [Kcap]
     int* counts = reinterpret_cast<int*>(score + a.Kcap);                   // [Kcap]
+    uint8_t* scode = reinterpret_cast<uint8_t*>(counts + a.Kcap);           // [T]
     __shared__ double lrate[2][kMaxRates];
     __shared__ float rev[2];
     __shared__ int s_site, s_a, s_b;
@@ -400,6 +477,7 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
         __syncthreads();
         const int s = s_site;
         if (s < 0) continue;
+        for (int c = threadIdx.x; c < d.T; c += blockDim.x) scode[c] = a.codes[(size_t)c * d.S + s];
         const float* sf = site_feat + (size_t)s * kSiteFeat;
         for (int k = warp; k < K; k += kGibbsWarps) {  // forward scores
             mlp_features(sf, spec + (size_t)k * kSpecStride + kSpecPi, counts[k], xs + warp * kMlpIn);
@@ -431,15 +509,18 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
             __syncthreads();
             continue;
         }
-        // Site likelihoods under the two classes (warps 0..R-1: a, R..2R-1: b),
-        // reverse scores with the updated class sizes (warps 2R, 2R+1).
-        if (warp < 2 * d.R) {
-            const int k = warp < d.R ? ca : cb, r = warp % d.R;
-            const double l = site_rate_lnl(a, i, s, r, spec + (size_t)k * kSpecStride,
-                                           ex + (size_t)k * d.N * d.R * kStates, stash);
-            if (lane == 0) lrate[warp < d.R ? 0 : 1][r] = l;
-        } else if (warp < 2 * d.R + 2) {
-            const int w = warp - 2 * d.R;
+        // Site likelihoods under the two classes (warps 0..nb-1: a, nb..2nb-1:
+        // b, kRateBlockLearned rates each), reverse scores with the updated
+        // class sizes (warps 2nb, 2nb+1).
+        const int nb = (d.R + kRateBlockLearned - 1) / kRateBlockLearned;
+        if (warp < 2 * nb) {
+            const int which = warp < nb ? 0 : 1, r0 = (warp % nb) * kRateBlockLearned;
+            const int k = which == 0 ? ca : cb;
+            site_class_lnl<kRateBlockLearned>(a, i, r0, spec + (size_t)k * kSpecStride,
+                                              ex + (size_t)k * d.N * d.R * kStates, stash, scode,
+                                              xch[warp], lrate[which] + r0);
+        } else if (warp < 2 * nb + 2) {
+            const int w = warp - 2 * nb;
             const int k = w == 0 ? ca : cb;
             mlp_features(sf, spec + (size_t)k * kSpecStride + kSpecPi, counts[k] + (w == 0 ? -1 : 1),
                          xs + warp * kMlpIn);
@@ -487,12 +568,12 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
 cudaError_t launch_learned_move(GibbsArgs a, const void* mlp, const float* site_feat, int32_t* n_acc,
                                 int32_t* n_prop, double* scratch, cudaStream_t st) {
     const Dims& d = a.d;
-    if (2 * d.R + 2 > kGibbsWarps) return cudaErrorInvalidValue;
     a.spec = scratch;
     a.expt = a.spec + (size_t)a.count * (a.Kcap + kAux) * kSpecStride;
     a.stash = a.expt + (size_t)a.count * (a.Kcap + kAux) * d.N * d.R * kStates;
     const size_t smem = ((kMlpParams * 2 + 15) & ~15) +
-                        sizeof(float) * (kGibbsWarps * (kMlpIn + kMlpHid) + a.Kcap) + sizeof(int) * a.Kcap;
+                        sizeof(float) * (kGibbsWarps * (kMlpIn + kMlpHid) + a.Kcap) + sizeof(int) * a.Kcap +
+                        d.T + 16;
     cudaError_t e = cudaFuncSetAttribute(learned_move_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
@@ -504,7 +585,7 @@ cudaError_t launch_learned_move(GibbsArgs a, const void* mlp, const float* site_
 size_t gibbs_scratch_doubles(const Dims& d, int count, int Kcap) {
     const size_t spec = (size_t)count * (Kcap + kAux) * kSpecStride;
     const size_t ex = (size_t)count * (Kcap + kAux) * d.N * d.R * kStates;
-    const size_t stash = (size_t)count * kGibbsWarps * d.NI * 32;
+    const size_t stash = (size_t)count * kGibbsWarps * d.NI * kRateBlock * 32;
     return spec + ex + stash;
 }
 
@@ -516,7 +597,7 @@ cudaError_t launch_gibbs(GibbsArgs a, double* scratch, cudaStream_t st) {
     a.expt = a.spec + (size_t)a.count * (a.Kcap + kAux) * kSpecStride;
     a.stash = a.expt + (size_t)a.count * (a.Kcap + kAux) * d.N * d.R * kStates;
     const size_t smem = sizeof(double) * (size_t)(a.Kcap + kAux) * (d.R + 1) +
-                        sizeof(int) * (a.Kcap + kAux) + 16;
+                        sizeof(int) * (a.Kcap + kAux) + d.T + 16;
     cudaError_t e = cudaFuncSetAttribute(gibbs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
