@@ -305,7 +305,7 @@ def test_every_kernel_variant_matches_oracle(cfg):
     eng.close()
 
 
-MIXED_ATOL = 1e-3  # |dlogL| per particle (nats) allowed for the FP32 path
+MIXED_ATOL = 3e-4  # |dlogL| per particle (nats) allowed for the FP32 path (sites <= 2,000)
 
 
 @pytest.mark.parametrize("cfg", SMALL, ids=lambda c: c.name)
