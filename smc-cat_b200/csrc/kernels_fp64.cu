@@ -585,11 +585,9 @@ cudaError_t launch_prune_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(prune_kernel<T, R, MINB, W, RB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    // All of L1 as shared memory, so that as many CTAs as the registers allow
-    // also fit their P buffers (four at 56 KB each).
-    e = cudaFuncSetAttribute(prune_kernel<T, R, MINB, W, RB>,
-                             cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
+    // The shared-memory carveout stays at the driver's choice: forcing the
+    // maximum (room for a fourth CTA's P buffers) measured slower, since the
+    // register-capped variants' spills then miss the smaller L1.
     prune_kernel<T, R, MINB, W, RB><<<ntiles, 32 * R, smem, st>>>(a);
     return cudaGetLastError();
 }
