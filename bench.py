@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--sweeps", type=int, default=2,
                     help="timed rejuvenation sweeps (0 to skip)")
     ap.add_argument("--sweep-temp", type=float, default=0.5)
+    ap.add_argument("--patterns", type=int, default=1,
+                    help="also time the same particles with site-pattern compression")
     ap.add_argument("--mixed", type=int, default=1,
                     help="also time the FP32 (mixed-precision) path on the same particles")
     ap.add_argument("--extra-configs", default="",
@@ -497,10 +499,44 @@ def main():
                  "autotune": tuned32}
         e32.close()
 
-    times = torch.tensor([ms, ms_e2e, ms_sweep, ms_mixed], dtype=torch.float64, device="cuda")
+    # ---- site-pattern compression (FP64) on the same particles -----------------
+    pat, ms_pat = None, 0.0
+    if args.patterns:
+        load()
+        eng.refresh(full=True)
+        ref64 = eng.lnl()
+        ep = smccat.Engine(codes, cfg.R, n, max_classes=st["logits"].shape[1], lg=cfg.lg,
+                           invar=cfg.invar, cat=cfg.cat, device=local, patterns=True)
+        ep.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                         st["logits"], st["assign"], st["pinv"], st["shape"])
+        ep.set_kernel_variant(tuned["variant"])
+        streamp = torch.cuda.ExternalStream(ep.stream_ptr, device=torch.device("cuda", local))
+        for _ in range(args.warmup):
+            ep.refresh(full=True)
+        barrier()
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record(streamp)
+        for _ in range(args.steps):
+            ep.refresh(full=True)
+        q1.record(streamp)
+        q1.synchronize()
+        barrier()
+        ms_pat = q0.elapsed_time(q1)
+        uniq = np.unique(codes.T, axis=0).shape[0]
+        pat = {"what": "each distinct alignment column evaluated once per particle and class, "
+                       "weighted by its site count (no counterpart in the reference)",
+               "distinct_columns": int(uniq), "sites": int(cfg.S),
+               "max_rel_dlogl_vs_uncompressed": float(np.max(np.abs(ep.lnl() - ref64) / np.abs(ref64)))}
+        ep.close()
+
+    times = torch.tensor([ms, ms_e2e, ms_sweep, ms_mixed, ms_pat], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    ms, ms_e2e, ms_sweep, ms_mixed = times.tolist()
+    ms, ms_e2e, ms_sweep, ms_mixed, ms_pat = times.tolist()
+    if pat is not None:
+        pat["value"] = units_per_step * args.steps * world / (ms_pat * 1e-3)
+        pat["unit"] = UNIT + " (every site counted)"
+        pat["ms_per_step"] = ms_pat / args.steps
     if mixed is not None:
         mixed["value"] = units_per_step * args.steps * world / (ms_mixed * 1e-3)
         mixed["unit"] = UNIT
@@ -566,6 +602,7 @@ def main():
             "kernel_ms_per_step": {k: v / args.steps for k, v in prof["ms"].items()},
             "gpu_launches": sum(prof["launches"].values()),
             "mixed_precision": mixed,
+            "site_patterns": pat,
             "sweeps_per_s": (args.sweeps / (ms_sweep * 1e-3)) if args.sweeps > 0 else None,
             "sweep": None if sweep_stats is None else {
                 "definition": f"Mcmc::operator() with {cfg.iterations} iterations on all {n} "

@@ -45,6 +45,14 @@ extern "C" {
 #define SMCCAT_MODEL_LG     1  /* LG exchangeabilities (else GTR, inferred)  */
 #define SMCCAT_MODEL_INVAR  2  /* +I invariant-site mixture                  */
 #define SMCCAT_MODEL_CAT    4  /* Dirichlet-process (CAT) class mixture      */
+#define SMCCAT_MODEL_PATTERNS 8 /* site-pattern compression (no counterpart in
+                                  the reference, which evaluates every site):
+                                  each particle evaluates every distinct
+                                  (alignment column, class) pair once and
+                                  weights it by its number of sites. Results
+                                  are the same up to rounding; per-site
+                                  log-likelihoods are still given for every
+                                  site                                        */
 
 /* precision */
 #define SMCCAT_PREC_FP64    0  /* plain FP64 pruning                         */

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "host_math.h"
@@ -90,6 +91,13 @@ struct smccat_ctx {
     bool tiles_dirty = false;
     int32_t* h_perm = nullptr;  // pinned staging for slot -> site maps
     Tile* h_tiles = nullptr;      // pinned staging for the tile list
+    // Site-pattern compression (SMCCAT_MODEL_PATTERNS): pattern id of every
+    // site (identical alignment columns share one), and per-slot site counts.
+    bool patterns = false;
+    std::vector<int32_t> pid;
+    int npat = 0;
+    int32_t* d_wt = nullptr;    // [P][S]
+    int32_t* h_wt = nullptr;    // pinned staging
     int32_t* h_tile_off = nullptr;
     std::vector<int> perm_dirty;
 
@@ -279,13 +287,14 @@ int smccat_destroy(smccat_ctx* c) {
     if (c->st) cudaStreamSynchronize(c->st);
     void* dptrs[] = {c->d_codes, c->d_isinv, c->d_invchar, c->d_perm, c->d_tiles, c->d_tile_off,
                      c->d_CL, c->d_LSC, c->d_Pm, c->d_spec, c->d_sws, c->d_partial, c->d_lnl,
-                     c->d_lnl_old, c->d_site_lnl, c->d_status, c->d_plan};
+                     c->d_lnl_old, c->d_site_lnl, c->d_status, c->d_plan, c->d_wt};
     for (void* p : dptrs) if (p) cudaFree(p);
     if (c->h_plan) cudaFreeHost(c->h_plan);
     if (c->h_sws) cudaFreeHost(c->h_sws);
     if (c->h_perm) cudaFreeHost(c->h_perm);
     if (c->h_tiles) cudaFreeHost(c->h_tiles);
     if (c->h_tile_off) cudaFreeHost(c->h_tile_off);
+    if (c->h_wt) cudaFreeHost(c->h_wt);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     if (c->plan_done) cudaEventDestroy(c->plan_done);
     if (c->st) cudaStreamDestroy(c->st);
@@ -341,6 +350,8 @@ int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** o
     A(&c->d_isinv, (size_t)S);
     A(&c->d_invchar, (size_t)S);
     A(&c->d_perm, (size_t)P * S);
+    c->patterns = (cfg->model_flags & SMCCAT_MODEL_PATTERNS) != 0;
+    if (c->patterns) A(&c->d_wt, (size_t)P * S);
     A(&c->d_tiles, (size_t)c->tile_cap);
     A(&c->d_tile_off, (size_t)P + 1);
     c->esz = (int)esz;
@@ -365,7 +376,9 @@ int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** o
         cudaMallocHost((void**)&c->h_sws, (size_t)P * K) != cudaSuccess ||
         cudaMallocHost((void**)&c->h_perm, (size_t)P * S * sizeof(int32_t)) != cudaSuccess ||
         cudaMallocHost((void**)&c->h_tiles, (size_t)c->tile_cap * sizeof(Tile)) != cudaSuccess ||
-        cudaMallocHost((void**)&c->h_tile_off, ((size_t)P + 1) * sizeof(int32_t)) != cudaSuccess) {
+        cudaMallocHost((void**)&c->h_tile_off, ((size_t)P + 1) * sizeof(int32_t)) != cudaSuccess ||
+        (c->patterns &&
+         cudaMallocHost((void**)&c->h_wt, (size_t)P * S * sizeof(int32_t)) != cudaSuccess)) {
         smccat_destroy(c);
         return fail(SMCCAT_ENOMEM, "pinned host allocation failed");
     }
@@ -378,6 +391,17 @@ int smccat_create(const smccat_config* cfg, const uint8_t* codes, smccat_ctx** o
 
     // Alignment-derived data (Particle.cpp:44-73).
     c->codes.assign(codes, codes + (size_t)T * S);
+    if (c->patterns) {  // pattern ids in order of first occurrence
+        std::unordered_map<std::string, int32_t> seen;
+        std::string col(T, '\0');
+        c->pid.resize(S);
+        for (int s = 0; s < S; ++s) {
+            for (int t = 0; t < T; ++t) col[t] = (char)codes[(size_t)t * S + s];
+            auto it = seen.emplace(col, (int32_t)seen.size()).first;
+            c->pid[s] = it->second;
+        }
+        c->npat = (int)seen.size();
+    }
     std::vector<double> isinv(S);
     std::vector<int32_t> invchar(S);
     for (int s = 0; s < S; ++s) {
@@ -499,10 +523,38 @@ int smccat_set_particles(smccat_ctx* c, int32_t first, int32_t count, const int3
         s.class_cnt.assign(cnt.begin() + 1, cnt.end());
         for (int k = 0; k < m.K; ++k) cnt[k + 1] += cnt[k];
         for (int x = 0; x < S; ++x) perm[cnt[s.assign[x]]++] = x;
+        if (c->patterns) {
+            // Within each class keep the first site of every pattern; its slot
+            // counts the class's sites with that column.
+            int32_t* wt = c->h_wt + (size_t)p * S;
+            std::vector<int32_t> slot_of(c->npat, -1), stamp(c->npat, -1);
+            s.site_rep.resize(S);
+            int out = 0, x0 = 0;
+            for (int k = 0; k < m.K; ++k) {
+                const int first_slot = out;
+                for (int q = x0; q < x0 + s.class_cnt[k]; ++q) {
+                    const int site = perm[q], pt = c->pid[site];
+                    if (stamp[pt] != k) {
+                        stamp[pt] = k;
+                        slot_of[pt] = out;
+                        perm[out] = site;
+                        wt[out] = 0;
+                        ++out;
+                    }
+                    wt[slot_of[pt]]++;
+                    s.site_rep[site] = perm[slot_of[pt]];
+                }
+                x0 += s.class_cnt[k];
+                s.class_cnt[k] = out - first_slot;
+            }
+        }
     }
     if (count > 0) {
         CK(h2d(c, c->d_perm + (size_t)first * S, c->h_perm + (size_t)first * S,
                (size_t)count * S * sizeof(int32_t)));
+        if (c->patterns)
+            CK(h2d(c, c->d_wt + (size_t)first * S, c->h_wt + (size_t)first * S,
+                   (size_t)count * S * sizeof(int32_t)));
         CK(cudaEventRecord(c->plan_done, c->st));
     }
     c->tiles_dirty = true;
@@ -704,6 +756,7 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
     a.nodes = reinterpret_cast<const NodeJob*>(c->d_plan + sizeof(PartHdr) * count);
     a.codes = c->d_codes;
     a.perm = c->d_perm;
+    a.wt = c->patterns ? c->d_wt : nullptr;
     a.Pm = c->d_Pm;
     a.spec = c->d_spec;
     a.sws = c->d_sws;
@@ -786,6 +839,10 @@ int smccat_get_site_lnl(smccat_ctx* c, int32_t p, double* out) {
     CK(cudaSetDevice(c->cfg.device));
     CK(d2h(c, out, c->d_site_lnl + (size_t)p * c->d.S, c->d.S * sizeof(double)));
     CK(cudaStreamSynchronize(c->st));
+    if (c->patterns) {  // only each slot's own site was written
+        const std::vector<int32_t>& rep = c->slots[p].site_rep;
+        for (int x = 0; x < c->d.S; ++x) out[x] = out[rep[x]];
+    }
     return SMCCAT_OK;
 }
 

@@ -38,7 +38,9 @@ struct Mirror {
 struct Slot {
     Mirror cur, old;
     std::vector<int32_t> assign;
-    std::vector<int32_t> class_cnt;  // sites per class, kept with `assign`
+    std::vector<int32_t> class_cnt;  // slots per class, kept with `assign`
+    std::vector<int32_t> site_rep;   // site-pattern compression: the site each site's
+                                     // slot evaluates (its value stands for this one)
     std::vector<uint8_t> dirty_cl, dirty_p, dirty_spec;
     bool loaded = false;
     bool full = false;          // next refresh rebuilds everything

@@ -19,6 +19,7 @@ struct PruneArgs {
     const NodeJob* nodes;
     const uint8_t* codes;
     const int32_t* perm;
+    const int32_t* wt;  // sites per slot [P][S] under site-pattern compression, else null
     const void* Pm;   // double, or float when fp32
     const double* spec;
     const uint8_t* sws;

@@ -529,7 +529,8 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
             }
             if (bad) u = NAN;
             a.site_lnl[(size_t)p * d.S + site[w]] = u;
-            v += u;
+            // A compressed slot stands for every site of its (column, class) pair.
+            v += a.wt ? u * a.wt[(size_t)p * d.S + tl.slot0 + q] : u;
         }
         v = warp_sum(v);
         if (lane == 0) a.partial[tile_id] = v;

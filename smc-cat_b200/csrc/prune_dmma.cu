@@ -363,6 +363,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_dmma_kernel(const PruneArg
             }
             if (bad) v = NAN;
             a.site_lnl[(size_t)p * d.S + st] = v;
+            if (a.wt) v *= a.wt[(size_t)p * d.S + tl.slot0 + lane];  // sites the slot stands for
         }
 #pragma unroll
         for (int o2 = 16; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o2);

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(_PKG_DIR, "lib", "libsmccat.so")
 HEADER_PATH = os.path.join(os.path.dirname(_PKG_DIR), "include", "smccat.h")
 
 OK, EINVAL, ECUDA, ENOMEM, ESTATE, ENUMERIC, ENODEV = range(7)
-MODEL_LG, MODEL_INVAR, MODEL_CAT = 1, 2, 4
+MODEL_LG, MODEL_INVAR, MODEL_CAT, MODEL_PATTERNS = 1, 2, 4, 8
 PREC_FP64, PREC_FP32 = 0, 1
 REFRESH_DIRTY, REFRESH_FULL = 0, 1
 
@@ -197,7 +197,7 @@ class Engine:
 
     def __init__(self, codes, num_rates: int, max_particles: int, max_classes: int = 1,
                  lg: bool = False, invar: bool = False, cat: bool = False, device: int = 0,
-                 precision: int = PREC_FP64):
+                 precision: int = PREC_FP64, patterns: bool = False):
         codes = np.ascontiguousarray(codes, dtype=np.uint8)
         self.T, self.S = codes.shape
         self.R = int(num_rates)
@@ -205,6 +205,7 @@ class Engine:
         self.P = int(max_particles)
         self.Kmax = int(max_classes)
         flags = (MODEL_LG if lg else 0) | (MODEL_INVAR if invar else 0) | (MODEL_CAT if cat else 0)
+        flags |= MODEL_PATTERNS if patterns else 0
         self.precision = int(precision)
         cfg = Config(self.T, self.S, self.R, self.P, self.Kmax, flags, self.precision, device)
         h = ctypes.c_void_p()
