@@ -239,6 +239,8 @@ int smccat_get_tuning(smccat_ctx* ctx, smccat_tuning* t);
 /* rateMatrixCholesky (Particle.hpp:93, set by main.cpp:267-289): lower
  * triangular 190 x 190, row-major; default 0.5 I. */
 int smccat_set_rate_cholesky(smccat_ctx* ctx, const double* lower190x190);
+/* The factor in use (190 x 190 row-major, zeros above the diagonal). */
+int smccat_get_rate_cholesky(smccat_ctx* ctx, double* lower190x190);
 
 /* Split posterior probabilities for the adaptive NNI move
  * (Tree::adaptiveNNIMove, Tree.cpp:673-766; computeSplitPosteriors,
@@ -261,6 +263,27 @@ int smccat_set_split_posteriors(smccat_ctx* ctx, int32_t n, const uint64_t* bits
 int smccat_compute_split_posteriors(smccat_ctx* ctx, int32_t first, int32_t count,
                                     const double* weights, int32_t cap, int32_t* n_out,
                                     uint64_t* bits, double* prob);
+
+/* The resampling and proposal-tuning half of an SMC step (main.cpp:176-301).
+ * Systematic resampling of [first, first+count) with the normalised weights
+ * norm_weights and a uniform draw u in [0, 1) (main.cpp:178-192, the same
+ * walk); ancestors[i] (relative to first) is the particle slot i descends from.
+ * Then, over the resampled population, the reference's proposal tuning
+ * (main.cpp:197-291), installed for smccat_propose / smccat_rejuvenate:
+ * shape_delta = max(0.5 var(log shape), 0.01); scale_delta =
+ * subtree_scale_delta = max(var(log branch length) over every non-root
+ * branch, 0.01); stationary_delta = max(var over every class's 20 logits, 0.01);
+ * invar_alpha = 0.5 mean(pinv) (+I models only); and without SMCCAT_MODEL_LG
+ * the exchangeability proposal: the uncentred X^T X of the resampled base
+ * vectors times 2.38^2/190 * 0.21, shrunk by 0.2 toward its mean diagonal,
+ * plus 1e-6 I, Cholesky-factored (SMCCAT_ENUMERIC if not positive definite),
+ * with rate_matrix_delta = max(shrinkage, 0.01). Variances are population
+ * variances. The split posteriors of the resampled population become the
+ * adaptive NNI table (T <= 128). With copy != 0 every slot then takes its
+ * ancestor's state (copyFromSerialized, main.cpp:299-301); the next refresh
+ * rebuilds the partials. */
+int smccat_resample_tune(smccat_ctx* ctx, int32_t first, int32_t count, const double* norm_weights,
+                         double u, int32_t copy, int32_t* ancestors);
 
 /* Particle::lnPrior (Particle.cpp:484-517) of the current states. */
 int smccat_ln_prior(smccat_ctx* ctx, int32_t first, int32_t count, double* out);

@@ -447,12 +447,139 @@ int smccat_set_rate_cholesky(smccat_ctx* c, const double* lower190) {
     return SMCCAT_OK;
 }
 
+int smccat_get_rate_cholesky(smccat_ctx* c, double* lower190) {
+    if (!c || !lower190) return mfail(SMCCAT_EINVAL, "null argument");
+    const auto& ch = tuning_of(c).chol;
+    std::copy(ch.begin(), ch.end(), lower190);
+    return SMCCAT_OK;
+}
+
 int smccat_set_split_posteriors(smccat_ctx* c, int32_t n, const uint64_t* bits, const double* prob) {
     if (!c || n < 0 || (n > 0 && (!bits || !prob))) return mfail(SMCCAT_EINVAL, "null argument");
     auto& mp = tuning_of(c).split_post;
     mp.clear();
     for (int i = 0; i < n; ++i) mp[Split{{bits[2 * i], bits[2 * i + 1]}}] = prob[i];
     return SMCCAT_OK;
+}
+
+int smccat_resample_tune(smccat_ctx* c, int32_t first, int32_t count, const double* w, double u,
+                         int32_t copy, int32_t* anc_out) {
+    if (!c || !w || !anc_out) return mfail(SMCCAT_EINVAL, "null argument");
+    if (first < 0 || count < 1) return mfail(SMCCAT_EINVAL, "bad range");
+    if (!(u >= 0.0 && u < 1.0)) return mfail(SMCCAT_EINVAL, "u must be in [0, 1)");
+    for (int i = 0; i < count; ++i)
+        if (!slot_of(c, first + i).loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
+    const Dims& d = dims_of(c);
+    const int flags = model_flags_of(c);
+    // Systematic resampling, main.cpp:178-192 (same walk, same arithmetic).
+    std::vector<int> a;
+    a.reserve(count);
+    {
+        double cumulative = w[0];
+        int k = 0;
+        double ruler = u / static_cast<double>(count);
+        const double step = 1.0 / static_cast<double>(count);
+        while ((int)a.size() < count) {
+            if (ruler <= cumulative) {
+                a.push_back(k);
+                ruler += step;
+            } else if (++k >= count) {
+                k = count - 1;
+                cumulative = 1.0;
+            } else {
+                cumulative += w[k];
+            }
+        }
+    }
+    // Proposal tuning over the resampled population, main.cpp:197-291.
+    // Variances are population variances (boost::accumulators tag::variance).
+    struct Var {
+        double n = 0, s = 0, s2 = 0;
+        void add(double x) { n += 1; s += x; s2 += x * x; }
+        double var() const { const double m = s / n; return s2 / n - m * m; }
+    } shape_v, branch_v, stat_v;
+    double pinv_mean = 0.0;
+    std::vector<double> xtx;
+    const bool gtr = !(flags & SMCCAT_MODEL_LG);
+    if (gtr) xtx.assign(kBase * kBase, 0.0);
+    for (int n : a) {
+        const Mirror& m = slot_of(c, first + n).cur;
+        shape_v.add(std::log(m.shape));
+        pinv_mean += m.pinv;
+        for (int x = 0; x < d.N; ++x)
+            if (x != m.root) branch_v.add(std::log(m.branch[x]));  // every non-root branch
+        for (int k = 0; k < m.K; ++k)
+            for (int j = 0; j < kStates; ++j) stat_v.add(m.logits[(size_t)k * kStates + j]);
+        if (gtr)  // X^T X of the base vectors, uncentred as in main.cpp:249
+            for (int i = 0; i < kBase; ++i)
+                for (int j = 0; j < kBase; ++j) xtx[i * kBase + j] += m.base[i] * m.base[j];
+    }
+    pinv_mean /= static_cast<double>(count);
+    Tuning& tn = tuning_of(c);
+    double shrink_diag = 0.0;
+    if (gtr) {
+        const double scale = (2.38 * 2.38) / 190.0 * 0.21, shrink = 0.2;
+        for (double& v : xtx) v *= scale;
+        for (int i = 0; i < kBase; ++i) shrink_diag += xtx[i * kBase + i];
+        shrink_diag = shrink_diag / 190.0 * shrink;
+        for (double& v : xtx) v *= 1.0 - shrink;
+        for (int i = 0; i < kBase; ++i) xtx[i * kBase + i] += shrink_diag + 1e-6;
+        // Cholesky (LLT), lower triangle in place.
+        for (int j = 0; j < kBase; ++j) {
+            double dj = xtx[j * kBase + j];
+            for (int k = 0; k < j; ++k) dj -= xtx[j * kBase + k] * xtx[j * kBase + k];
+            if (!(dj > 0.0)) return mfail(SMCCAT_ENUMERIC, "rate-matrix covariance is not positive definite");
+            dj = std::sqrt(dj);
+            xtx[j * kBase + j] = dj;
+            for (int i = j + 1; i < kBase; ++i) {
+                double v = xtx[i * kBase + j];
+                for (int k = 0; k < j; ++k) v -= xtx[i * kBase + k] * xtx[j * kBase + k];
+                xtx[i * kBase + j] = v / dj;
+            }
+        }
+        for (int i = 0; i < kBase; ++i)
+            for (int j = i + 1; j < kBase; ++j) xtx[i * kBase + j] = 0.0;
+        tn.chol = xtx;
+        tn.t.rate_matrix_delta = std::max(shrink_diag, 0.01);
+    }
+    tn.t.shape_delta = std::max(0.5 * shape_v.var(), 0.01);
+    tn.t.scale_delta = std::max(branch_v.var(), 0.01);
+    tn.t.subtree_scale_delta = tn.t.scale_delta;
+    tn.t.stationary_delta = std::max(stat_v.var(), 0.01);
+    if ((flags & SMCCAT_MODEL_INVAR) && pinv_mean > 0.0) tn.t.invar_alpha = pinv_mean * 0.5;
+    // computeSplitPosteriors over the assignments (main.cpp:203-207).
+    std::vector<double> mult(count, 0.0);
+    for (int n : a) mult[n] += 1.0 / static_cast<double>(count);
+    int32_t nsplit = 0;
+    if (d.T <= 128) {
+        const int rc = smccat_compute_split_posteriors(c, first, count, mult.data(), 0, &nsplit, nullptr,
+                                                       nullptr);
+        if (rc) return rc;
+    }
+    for (int i = 0; i < count; ++i) anc_out[i] = a[i];
+    if (!copy) return SMCCAT_OK;
+    // copyFromSerialized of each ancestor into its new slot (main.cpp:299-301).
+    const size_t N = d.N, S = d.S, K = d.Kmax;
+    std::vector<int32_t> par(count * N), nk(count), asg(count * S);
+    std::vector<double> br(count * N), base(count * kBase), lg(count * K * kStates), pv(count), sh(count);
+    int rc = smccat_get_particles(c, first, count, par.data(), br.data(), base.data(), nk.data(), lg.data(),
+                                  asg.data(), pv.data(), sh.data());
+    if (rc) return rc;
+    std::vector<int32_t> par2(count * N), nk2(count), asg2(count * S);
+    std::vector<double> br2(count * N), base2(count * kBase), lg2(count * K * kStates), pv2(count), sh2(count);
+    for (int i = 0; i < count; ++i) {
+        const int f = a[i];
+        std::copy(&par[f * N], &par[f * N] + N, &par2[i * N]);
+        std::copy(&br[f * N], &br[f * N] + N, &br2[i * N]);
+        std::copy(&base[f * kBase], &base[f * kBase] + kBase, &base2[i * kBase]);
+        std::copy(&lg[f * K * kStates], &lg[f * K * kStates] + K * kStates, &lg2[i * K * kStates]);
+        std::copy(&asg[f * S], &asg[f * S] + S, &asg2[i * S]);
+        nk2[i] = nk[f];
+        pv2[i] = pv[f];
+        sh2[i] = sh[f];
+    }
+    return smccat_set_particles(c, first, count, par2.data(), br2.data(), base2.data(), nk2.data(),
+                                lg2.data(), asg2.data(), pv2.data(), sh2.data());
 }
 
 int smccat_compute_split_posteriors(smccat_ctx* c, int32_t first, int32_t count,

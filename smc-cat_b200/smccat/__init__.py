@@ -133,6 +133,8 @@ def lib():
         "smccat_compute_split_posteriors": ([vp, _i32, _i32, _dp, _i32, _ip,
                                              ctypes.POINTER(ctypes.c_uint64), _dp], ctypes.c_int),
         "smccat_ln_prior": ([vp, _i32, _i32, _dp], ctypes.c_int),
+        "smccat_resample_tune": ([vp, _i32, _i32, _dp, ctypes.c_double, _i32, _ip], ctypes.c_int),
+        "smccat_get_rate_cholesky": ([vp, _dp], ctypes.c_int),
         "smccat_propose": ([vp, _i32, _i32, ctypes.c_uint64, _ip, _dp], ctypes.c_int),
         "smccat_rejuvenate": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64,
                                ctypes.POINTER(MoveStats)], ctypes.c_int),
@@ -363,6 +365,20 @@ class Engine:
             bits.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), prob.ctypes.data_as(_dp)))
         m = min(cap, n.value)
         return bits[:m], prob[:m]
+
+    def rate_cholesky(self) -> np.ndarray:
+        out = np.zeros((190, 190))
+        _check(lib().smccat_get_rate_cholesky(self._h, out.ctypes.data_as(_dp)))
+        return out
+
+    def resample_tune(self, norm_weights, u, copy=True, first=0) -> np.ndarray:
+        """Systematic resampling + the reference's proposal tuning; returns the
+        ancestor of every slot of [first, first + len(norm_weights))."""
+        w, wp = _d(norm_weights)
+        anc = np.zeros(len(w), dtype=np.int32)
+        _check(lib().smccat_resample_tune(self._h, int(first), len(w), wp, float(u),
+                                          1 if copy else 0, anc.ctypes.data_as(_ip)))
+        return anc
 
     def ln_prior(self, first=0, count=None) -> np.ndarray:
         count = self.P - first if count is None else count

@@ -98,3 +98,19 @@ def test_two_rank_exchange_with_gloo():
         assert uniform
         # destination slot d of rank r now holds the state of particle assign[d]
         assert vals == [float(assign[r * per_rank + i]) for i in range(per_rank)]
+
+
+def test_oracle_resampling_agrees_with_the_distributed_module():
+    """Both restate main.cpp:178-192; uniform weights keep every particle once,
+    a point mass copies one particle everywhere."""
+    from oracle import tuning
+    from smccat import distributed
+    rng = np.random.default_rng(2)
+    for _ in range(20):
+        n = int(rng.integers(1, 40))
+        w = rng.random(n)
+        w /= w.sum()
+        u = float(rng.random())
+        assert list(distributed.systematic_resample(w, u)) == tuning.systematic_resample(w, u)
+    assert tuning.systematic_resample(np.full(8, 1 / 8), 0.5) == list(range(8))
+    assert tuning.systematic_resample(np.eye(5)[3], 0.2) == [3] * 5

@@ -359,3 +359,35 @@ def test_split_posteriors_match_oracle_and_drive_adaptive_nni():
         eng.accept(np.zeros(CFG.particles, np.uint8))
     assert seen >= 5
     eng.close()
+
+
+def test_resample_tune_matches_oracle():
+    """Systematic resampling and proposal tuning of the SMC step
+    (main.cpp:176-301) against oracle/tuning.py; every slot then carries its
+    ancestor's state and, after a refresh, its ancestor's log-likelihood."""
+    from oracle import tuning
+    eng, codes, st = engine()
+    n = CFG.particles
+    before = eng.get_particles()
+    lnl0 = eng.lnl()
+    w = np.random.default_rng(21).random(n) ** 3
+    w /= w.sum()
+    u = 0.37
+    anc = eng.resample_tune(w, u, copy=True)
+    ref_anc = tuning.systematic_resample(w, u)
+    np.testing.assert_array_equal(anc, ref_anc)
+    ref = tuning.tune(before, ref_anc, gtr=not CFG.lg)
+    t = eng.tuning()
+    for k in ("shape_delta", "scale_delta", "stationary_delta", "rate_matrix_delta"):
+        assert t[k] == pytest.approx(ref[k], rel=1e-11), k
+    assert t["subtree_scale_delta"] == t["scale_delta"]
+    assert t["invar_alpha"] == pytest.approx(0.5 * ref["pinv_mean"], rel=1e-12)
+    np.testing.assert_allclose(eng.rate_cholesky(), ref["cholesky"], rtol=1e-9, atol=1e-12)
+    after = eng.get_particles()
+    for i in range(n):
+        np.testing.assert_array_equal(after["parent"][i], before["parent"][anc[i]])
+        np.testing.assert_array_equal(after["assign"][i], before["assign"][anc[i]])
+        np.testing.assert_array_equal(after["branch"][i], before["branch"][anc[i]])
+    eng.refresh()
+    np.testing.assert_allclose(eng.lnl(), lnl0[anc], rtol=1e-12)
+    eng.close()
