@@ -68,6 +68,16 @@ def parse():
                     help="comma-separated CAT configs (e.g. 3,4) to time in particle waves")
     ap.add_argument("--extra-particles", type=int, default=0,
                     help="particles for --extra-configs (default: the configuration's)")
+    ap.add_argument("--sampler-config", type=int, default=0,
+                    help="CAT config (e.g. 4) on which to compare sampler sweeps/s: plain FP64 + "
+                         "Gibbs against FP32 + learned proposal (0 to skip)")
+    ap.add_argument("--sampler-particles", type=int, default=32)
+    ap.add_argument("--sampler-sweeps", type=int, default=1)
+    ap.add_argument("--smc", type=int, default=0,
+                    help="run whole SMC analyses (temperature 0 -> 1) on a 16-taxon x 500-site "
+                         "CAT workload: plain FP64 + Gibbs against FP32 + learned proposal, "
+                         "this many replicate seeds each")
+    ap.add_argument("--smc-particles", type=int, default=64)
     ap.add_argument("--gibbs-particles", type=int, default=32,
                     help="particles of a CAT --extra-configs run timed through one Gibbs pass "
                          "and one learned-proposal pass (0 to skip)")
@@ -238,6 +248,111 @@ def measure_reassignment(codes, st, cfg, n, local, torch):
             "learned": {"train_seconds": t2 - t1, "train_loss": loss, "seconds": t3 - t2,
                         "site_updates_per_s": n * its / (t3 - t2),
                         "acceptance": ls["accepted"] / max(ls["proposed"], 1)}}
+
+
+def measure_sampler(cid, n, sweeps, local, torch):
+    """Sampler sweeps/s on a CAT configuration. One sweep = Mcmc::operator()
+    with the configuration's iterations on every particle (lockstep) + one CAT
+    reassignment pass of floor(S/2) site updates per particle. Plain arm: FP64
+    partials, Gibbs (Neal 8). Chosen arm: FP32 partials, the learned proposal,
+    its MLP trained (untimed) on the assignments one Gibbs warm-up pass leaves.
+    The chosen arm's final states are re-evaluated in FP64 for its |dlogL|.
+    Wall clock around device-synchronised calls."""
+    import smccat
+    from smccat import workload
+    cfg = workload.CONFIGS[cid]
+    codes, _ = workload.simulate_alignment(cfg, np.random.default_rng(cfg.seed))
+    st = workload.make_particles(cfg, n, np.random.default_rng(cfg.seed * 7 + 1))
+    kmax = st["logits"].shape[1] + 32
+    logits = np.zeros((n, kmax, 20))
+    logits[:, :st["logits"].shape[1]] = st["logits"]
+    res = {"workload": cfg.name, "particles": n, "sweeps": sweeps,
+           "sweep": f"Mcmc::operator() x {cfg.iterations} iterations + {cfg.S // 2} site updates "
+                    "per particle, temperature 1"}
+    engines = {}
+    for arm, prec in (("plain_fp64_gibbs", smccat.PREC_FP64), ("fp32_learned", smccat.PREC_FP32)):
+        eng = smccat.Engine(codes, cfg.R, n, max_classes=kmax, lg=cfg.lg, invar=cfg.invar,
+                            cat=cfg.cat, device=local, precision=prec)
+        eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"], logits,
+                          st["assign"], st["pinv"], st["shape"])
+        eng.refresh(full=True)
+        info = {}
+        if arm == "fp32_learned":
+            eng.gibbs(temperature=1.0, seed=1)
+            info["train_loss"] = eng.learned_train(epochs=1, batch_sites=512, lr=1e-3, seed=2,
+                                                   first=0, count=min(n, 8))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        steps, acc = 0, []
+        for k in range(sweeps):
+            r = eng.rejuvenate(iterations=cfg.iterations, temperature=1.0, seed=100 + k)
+            steps += r["lockstep_steps"]
+            if arm == "plain_fp64_gibbs":
+                eng.gibbs(temperature=1.0, seed=200 + k)
+            else:
+                g = eng.learned_move(updates=cfg.S // 2, temperature=1.0, seed=200 + k)
+                acc.append(g["accepted"] / max(g["proposed"], 1))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        info.update({"sweeps_per_s": sweeps / (t1 - t0), "seconds_per_sweep": (t1 - t0) / sweeps,
+                     "lockstep_steps_per_sweep": steps / sweeps})
+        if acc:
+            info["learned_acceptance"] = float(np.mean(acc))
+        res[arm] = info
+        engines[arm] = eng
+    # FP64 re-evaluation of the chosen arm's final states.
+    e32, e64 = engines["fp32_learned"], engines["plain_fp64_gibbs"]
+    l32 = e32.lnl()
+    g = e32.get_particles()
+    e64.set_particles(0, g["parent"], g["branch"], g["base"], g["num_classes"], g["logits"],
+                      g["assign"], g["pinv"], g["shape"])
+    e64.refresh(full=True)
+    res["fp32_learned"]["max_abs_dlogl_vs_fp64"] = float(np.max(np.abs(l32 - e64.lnl())))
+    for e in engines.values():
+        e.close()
+    res["speedup_sweeps_per_s"] = res["fp32_learned"]["sweeps_per_s"] / res["plain_fp64_gibbs"]["sweeps_per_s"]
+    return res
+
+
+def measure_smc(reps, n, local, torch):
+    """Whole SMC analyses (main.cpp:147-336 through smccat.smc.run) from the
+    same initial population, per arm and replicate seed: log marginal
+    likelihood, SMC steps, resampling rounds, wall seconds, final ESS per
+    second. The initial population comes from the workload generator, not
+    from the prior, so log Z is compared between arms, not to a truth."""
+    import smccat
+    from smccat import smc, workload
+    cfg = workload.WorkloadConfig("cat_gtr_g4_16x500", T=16, S=500, R=4, particles=n,
+                                  iterations=5, lg=False, invar=False, cat=True, alpha=0.8,
+                                  dp_concentration=3.0, k_range=(1, 6), seed=9)
+    codes, _ = workload.simulate_alignment(cfg, np.random.default_rng(cfg.seed))
+    st = workload.make_particles(cfg, n, np.random.default_rng(99))
+    kmax = st["logits"].shape[1] + 24
+    logits = np.zeros((n, kmax, 20))
+    logits[:, :st["logits"].shape[1]] = st["logits"]
+    out = {"workload": cfg.name, "particles": n, "rejuvenation_iterations": cfg.iterations,
+           "threshold": 0.6, "alg8_probability": 0.1}
+    for arm, prec, move in (("plain_fp64_gibbs", smccat.PREC_FP64, "gibbs"),
+                            ("fp32_learned", smccat.PREC_FP32, "learned")):
+        runs = []
+        for r in range(reps):
+            eng = smccat.Engine(codes, cfg.R, n, max_classes=kmax, lg=cfg.lg, invar=cfg.invar,
+                                cat=cfg.cat, device=local, precision=prec)
+            eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                              logits, st["assign"], st["pinv"], st["shape"])
+            eng.refresh(full=True)
+            res = smc.run(eng, cat=True, iterations=cfg.iterations, reassign=move, seed=1000 + r,
+                          sync=torch.cuda.synchronize)
+            res.pop("temperatures")
+            runs.append(res)
+            eng.close()
+        lz = np.array([x["log_z"] for x in runs])
+        out[arm] = {"runs": runs, "log_z_mean": float(lz.mean()),
+                    "log_z_sd": float(lz.std(ddof=1)) if reps > 1 else None,
+                    "seconds_mean": float(np.mean([x["seconds"] for x in runs])),
+                    "final_ess_per_s_mean": float(np.mean([x["final_ess_per_s"] for x in runs]))}
+    out["speedup_wall"] = out["plain_fp64_gibbs"]["seconds_mean"] / out["fp32_learned"]["seconds_mean"]
+    return out
 
 
 def measure_config_waves(cid, steps, local, rank, particles=0, oracle_sample=2, gibbs_particles=0):
@@ -619,6 +734,11 @@ def main():
                                      particles=args.extra_particles,
                                      gibbs_particles=args.gibbs_particles)
                 for c in args.extra_configs.split(",") if c.strip()]
+        if args.smc:
+            line["smc"] = measure_smc(args.smc, args.smc_particles, local, torch)
+        if args.sampler_config:
+            line["sampler"] = measure_sampler(args.sampler_config, args.sampler_particles,
+                                              args.sampler_sweeps, local, torch)
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(cfg, codes, st, args.cpu_sample)
         print(json.dumps(line), flush=True)
