@@ -812,6 +812,44 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
 }
 
 const Slot& smccat::slot_of(const smccat_ctx* c, int p) { return c->slots[p]; }
+Slot& smccat::slot_mut(smccat_ctx* c, int p) { return c->slots[p]; }
+
+int smccat::device_view(smccat_ctx* c, int first, int count, DeviceView* v) {
+    if (c->tiles_dirty) return fail(SMCCAT_ESTATE, "refresh the particles first");
+    const Dims& d = c->d;
+    PruneArgs& a = v->pa;
+    a = PruneArgs{};
+    a.d = d;
+    a.first = first;
+    a.tile_begin = c->tile_off[first];
+    a.tiles = c->d_tiles;
+    a.codes = c->d_codes;
+    a.perm = c->d_perm;
+    a.wt = c->patterns ? c->d_wt : nullptr;
+    a.Pm = c->d_Pm;
+    a.spec = c->d_spec;
+    a.sws = c->d_sws;
+    a.isinv = c->d_isinv;
+    a.invchar = c->d_invchar;
+    a.CL = c->d_CL;
+    a.fp32 = c->esz == 4;
+    a.LSC = c->d_LSC;
+    a.site_lnl = c->d_site_lnl;
+    a.partial = c->d_partial;
+    a.status = c->d_status;
+    v->ntiles = c->tile_off[first + count] - c->tile_off[first];
+    v->variant = c->prune_variant;
+    v->lnl = c->d_lnl;
+    v->lnl_old = c->d_lnl_old;
+    v->tile_off = c->d_tile_off;
+    v->sws = c->d_sws;
+    v->spec = c->d_spec;
+    v->Pm = c->d_Pm;
+    v->fp32 = c->esz == 4;
+    v->status = c->d_status;
+    v->st = c->st;
+    return SMCCAT_OK;
+}
 const Dims& smccat::dims_of(const smccat_ctx* c) { return c->d; }
 int smccat::model_flags_of(const smccat_ctx* c) { return c->cfg.model_flags; }
 const double* smccat::lnl_device(const smccat_ctx* c) { return c->d_lnl; }

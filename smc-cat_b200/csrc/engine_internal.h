@@ -71,4 +71,25 @@ void learned_release(const smccat_ctx* c);
 // BF16 MLP parameters and the device site features, or null if untrained.
 const void* learned_inference_weights(const smccat_ctx* c, const float** site_feat);
 
+// Device buffers of a particle range for kernels launched outside
+// refresh_internal (the device-side moves): a pruning argument block with
+// everything but hdr / nodes filled in, the launch shape, and what the
+// transition-matrix and reduction kernels read. Needs a current tile list.
+struct DeviceView {
+    PruneArgs pa;
+    int ntiles = 0, variant = 0;
+    double* lnl = nullptr;
+    double* lnl_old = nullptr;
+    const int32_t* tile_off = nullptr;  // device
+    const uint8_t* sws = nullptr;
+    const double* spec = nullptr;
+    void* Pm = nullptr;
+    bool fp32 = false;
+    int* status = nullptr;
+    cudaStream_t st = nullptr;
+};
+int device_view(smccat_ctx* c, int first, int count, DeviceView* v);
+// Mutable host mirror of one slot (the device-side moves write their results back).
+Slot& slot_mut(smccat_ctx* c, int p);
+
 }  // namespace smccat

@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
                                                           const double* __restrict__ spec,
                                                           T* __restrict__ Pm, Dims d) {
     const PmJob mj = mjobs[blockIdx.x];
+    if (mj.nj <= 0) return;  // fixed-shape job grids (device-side moves) leave empty entries
     const PartHdr* h = hdr + mj.i;
     const int p = first + mj.i;
     // Rows in 4-column-block interleaved order (pm_ilv): the pair loads of a

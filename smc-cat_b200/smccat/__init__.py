@@ -135,6 +135,8 @@ def lib():
         "smccat_ln_prior": ([vp, _i32, _i32, _dp], ctypes.c_int),
         "smccat_resample_tune": ([vp, _i32, _i32, _dp, ctypes.c_double, _i32, _ip], ctypes.c_int),
         "smccat_get_rate_cholesky": ([vp, _dp], ctypes.c_int),
+        "smccat_branch_sweep": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64, _i32,
+                                 ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "smccat_propose": ([vp, _i32, _i32, ctypes.c_uint64, _ip, _dp], ctypes.c_int),
         "smccat_rejuvenate": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64,
                                ctypes.POINTER(MoveStats)], ctypes.c_int),
@@ -365,6 +367,16 @@ class Engine:
             bits.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), prob.ctypes.data_as(_dp)))
         m = min(cap, n.value)
         return bits[:m], prob[:m]
+
+    def branch_sweep(self, steps, temperature, seed, use_graph=True, first=0, count=None) -> dict:
+        """Branch-length MCMC steps entirely on the device (one CUDA graph)."""
+        count = self.P - first if count is None else count
+        st = np.zeros(4, dtype=np.int64)
+        _check(lib().smccat_branch_sweep(self._h, int(first), int(count), int(steps),
+                                         float(temperature), int(seed), 1 if use_graph else 0,
+                                         st.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return {"branch_proposed": int(st[0]), "branch_accepted": int(st[1]),
+                "subtree_proposed": int(st[2]), "subtree_accepted": int(st[3])}
 
     def rate_cholesky(self) -> np.ndarray:
         out = np.zeros((190, 190))
