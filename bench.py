@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--sweeps", type=int, default=2,
                     help="timed rejuvenation sweeps (0 to skip)")
     ap.add_argument("--sweep-temp", type=float, default=0.5)
+    ap.add_argument("--branch-steps", type=int, default=50,
+                    help="device-side branch-length MH steps timed as one graph (0 to skip)")
     ap.add_argument("--patterns", type=int, default=1,
                     help="also time the same particles with site-pattern compression")
     ap.add_argument("--mixed", type=int, default=1,
@@ -578,6 +580,24 @@ def main():
         s1.synchronize()
         barrier()
         ms_sweep = s0.elapsed_time(s1)
+    # ---- branch-length sweep with everything on the device (one CUDA graph) ----
+    dev_sweep, ms_dev = None, 0.0
+    if args.sweeps > 0 and args.branch_steps > 0:
+        load()
+        eng.refresh(full=True)
+        eng.branch_sweep(steps=4, temperature=args.sweep_temp, seed=5 + rank)
+        barrier()
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        d0.record(stream)
+        bst = eng.branch_sweep(steps=args.branch_steps, temperature=args.sweep_temp, seed=6 + rank)
+        d1.record(stream)
+        d1.synchronize()
+        barrier()
+        ms_dev = d0.elapsed_time(d1)
+        dev_sweep = {"what": "scaleBranch / scaleSubtree MH steps on every particle, proposals, plans "
+                             "and accept/reject on the device, captured as one CUDA graph "
+                             "(upload, capture and sync-back included)",
+                     "steps": args.branch_steps, **bst}
 
     # ---- mixed precision (FP32 partials / matrices) on the same particles ----------
     mixed, ms_mixed = None, 0.0
@@ -644,10 +664,15 @@ def main():
                "max_rel_dlogl_vs_uncompressed": float(np.max(np.abs(ep.lnl() - ref64) / np.abs(ref64)))}
         ep.close()
 
-    times = torch.tensor([ms, ms_e2e, ms_sweep, ms_mixed, ms_pat], dtype=torch.float64, device="cuda")
+    times = torch.tensor([ms, ms_e2e, ms_sweep, ms_mixed, ms_pat, ms_dev], dtype=torch.float64,
+                         device="cuda")
     if dist is not None:
         dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    ms, ms_e2e, ms_sweep, ms_mixed, ms_pat = times.tolist()
+    ms, ms_e2e, ms_sweep, ms_mixed, ms_pat, ms_dev = times.tolist()
+    if dev_sweep is not None:
+        dev_sweep["ms_per_step"] = ms_dev / args.branch_steps
+        if sweep_stats is not None and sweep_stats["lockstep_steps"]:
+            dev_sweep["host_driven_ms_per_lockstep_step"] = ms_sweep / args.sweeps / sweep_stats["lockstep_steps"]
     if pat is not None:
         pat["value"] = units_per_step * args.steps * world / (ms_pat * 1e-3)
         pat["unit"] = UNIT + " (every site counted)"
@@ -718,6 +743,7 @@ def main():
             "gpu_launches": sum(prof["launches"].values()),
             "mixed_precision": mixed,
             "site_patterns": pat,
+            "device_branch_sweep": dev_sweep,
             "sweeps_per_s": (args.sweeps / (ms_sweep * 1e-3)) if args.sweeps > 0 else None,
             "sweep": None if sweep_stats is None else {
                 "definition": f"Mcmc::operator() with {cfg.iterations} iterations on all {n} "
