@@ -285,18 +285,19 @@ int smccat_compute_split_posteriors(smccat_ctx* ctx, int32_t first, int32_t coun
 int smccat_resample_tune(smccat_ctx* ctx, int32_t first, int32_t count, const double* norm_weights,
                          double u, int32_t copy, int32_t* ancestors);
 
-/* Branch-length rejuvenation with everything on the device: `steps` lockstep
- * Metropolis-Hastings steps of Tree::scaleBranchMove / Tree::scaleSubtreeMove
- * (Tree.cpp:553-612, in their 0.4 : 0.1 proportion of Particle::treeMove,
- * Particle.cpp:682-701) on every particle of [first, first+count), at
- * `temperature`, with the tuned scale_delta / subtree_scale_delta. Each step's
- * proposal, dirty-node plan, transition matrices, pruning, reduction and
- * accept/reject run as device kernels with fixed launch shapes; with
- * use_graph != 0 the whole sweep is captured as one CUDA graph and launched
- * once. Draws come from a Philox stream per particle seeded by `seed`.
- * Afterwards the host state holds the final branch lengths (topology moves stay
- * with smccat_rejuvenate). Needs refreshed, committed particles. stats (may be
- * NULL): proposed / accepted scaleBranch, proposed / accepted scaleSubtree. */
+/* Tree rejuvenation with everything on the device: `steps` lockstep
+ * Metropolis-Hastings steps of Tree::scaleBranchMove, Tree::scaleSubtreeMove
+ * and Tree::NNIMove (Tree.cpp:553-671, in their 0.4 : 0.1 : 0.1 proportion of
+ * Particle::treeMove, Particle.cpp:682-701) on every particle of
+ * [first, first+count), at `temperature`, with the tuned scale_delta /
+ * subtree_scale_delta. Each step's proposal, dirty-node plan, transition
+ * matrices, pruning, reduction and accept/reject run as device kernels with
+ * fixed launch shapes; with use_graph != 0 the whole sweep is captured as one
+ * CUDA graph and launched once. Draws come from a Philox stream per particle
+ * seeded by `seed`. Afterwards the host state holds the final trees and branch
+ * lengths (adaptive NNI and SPR stay with smccat_rejuvenate). Needs refreshed,
+ * committed particles. stats (may be NULL, else 6 entries): proposed /
+ * accepted scaleBranch, scaleSubtree, NNI. */
 int smccat_branch_sweep(smccat_ctx* ctx, int32_t first, int32_t count, int32_t steps,
                         double temperature, uint64_t seed, int32_t use_graph, int64_t* stats);
 

@@ -1,30 +1,33 @@
-// Branch-length rejuvenation on the device, captured as one CUDA graph.
+// Tree moves on the device, a whole sweep captured as one CUDA graph.
 //
 // The host MCMC driver (mcmc.cu) proposes every move on host mirrors and packs
-// each step's plan on the host. Here the two branch-length moves of the
-// reference's tree-move mixture -- Tree::scaleBranchMove and
-// Tree::scaleSubtreeMove (Tree.cpp:553-612; 0.4 and 0.1 of Particle::treeMove,
-// Particle.cpp:682-701, so 80% / 20% of these steps) -- run for every particle
-// of a range in lockstep with nothing on the host between steps:
+// each step's plan on the host. Here three moves of the reference's tree-move
+// mixture -- Tree::scaleBranchMove, Tree::scaleSubtreeMove (Tree.cpp:553-612)
+// and Tree::NNIMove (Tree.cpp:625-671), 0.4, 0.1 and 0.1 of
+// Particle::treeMove (Particle.cpp:682-701), so 4 : 1 : 1 here -- run for
+// every particle of a range in lockstep with nothing on the host between steps:
 //
 //   dm_propose_kernel   one thread per particle: Philox draws, the array edit of
-//                       the flattened tree's branch lengths, the dirty sets
-//                       (the scaled nodes' transition matrices; the subtree's
-//                       internal partials and every ancestor of the scaled
-//                       node), the plan in post-order with the next workspaces,
-//                       the tree-length prior change and the log Hastings ratio;
+//                       the flattened tree (branch lengths, or for NNI the
+//                       swap of one child of x with x's sibling in the parent
+//                       and child tables), the dirty sets (scaled nodes'
+//                       transition matrices; the subtree's internal partials,
+//                       or x for NNI, and every ancestor), the plan in
+//                       post-order with the next workspaces, the tree-length
+//                       prior change and the log Hastings ratio;
 //   pmat_kernel, prune_kernel, reduce_kernel
 //                       the engine's kernels on that device-built plan, with
 //                       launch shapes fixed by the range (empty job slots exit);
 //   dm_mh_kernel        one thread per particle: Metropolis-Hastings on
 //                       temperature * lnL + lnPrior + log Hastings (Mcmc.cpp:57-60);
 //                       accept commits the new workspaces, reject restores the
-//                       branch lengths (the dirty work sits in the other
-//                       workspace, as on the host path).
+//                       branch lengths or the parent / child tables (the dirty
+//                       work sits in the other workspace, as on the host path).
 //
 // A sweep of B steps is B repetitions of this fixed sequence, captured into a
 // CUDA graph and launched once. At the end the host mirrors take the final
-// branch lengths and committed workspaces back.
+// trees (children and post-order regenerated from the parent tables), branch
+// lengths and committed workspaces back.
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
 #include <math.h>
@@ -48,6 +51,7 @@ struct DmArgs {
     int first, count, nchunk;
     int32_t* parent;     // [count][N]
     int32_t* kids;       // [count][2N]
+    int32_t* nni;        // [count][6] x, a, n1, n2 and their child-slot indices
     double* branch;      // [count][N]
     uint8_t* clws;       // [count][N] committed partial workspace of each node
     uint8_t* pws;        // [count][N] committed transition-matrix workspace
@@ -58,7 +62,7 @@ struct DmArgs {
     int32_t* undo_node;  // [count][N] scaled nodes, walk order
     double* undo_len;    // [count][N] their previous lengths
     int32_t* nundo;      // [count]
-    int32_t* kind;       // [count] 0 scaleBranch, 1 scaleSubtree
+    int32_t* kind;       // [count] 0 scaleBranch, 1 scaleSubtree, 2 NNI
     double* extra;       // [count] lnPrior change + log Hastings ratio
     const PartHdr* hdr0; // [count] root, classes, pinv, rates
     PartHdr* hdr;        // [count] this step's
@@ -68,7 +72,7 @@ struct DmArgs {
     curandStatePhilox4_32_10_t* rng;  // [count]
     double* lnl;         // engine arrays, [max_particles]
     double* lnl_old;
-    unsigned long long* stats;  // proposed / accepted, per kind
+    unsigned long long* stats;  // proposed / accepted, per kind (6)
     double scale_delta, subtree_delta, temp;
 };
 
@@ -82,8 +86,8 @@ __global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
     if (i >= a.count) return;
     const Dims& d = a.d;
     const int N = d.N, T = d.T, NI = d.NI;
-    const int32_t* par = a.parent + (size_t)i * N;
-    const int32_t* kids = a.kids + (size_t)i * 2 * N;
+    int32_t* par = a.parent + (size_t)i * N;
+    int32_t* kids = a.kids + (size_t)i * 2 * N;
     double* br = a.branch + (size_t)i * N;
     uint8_t* dirty = a.dirty + (size_t)i * N;
     int32_t* stk = a.stack + (size_t)i * N;
@@ -98,16 +102,40 @@ __global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
         dirty[n] = 0;
         L0 += br[n];
     }
-    const bool subtree = curand_uniform_double(&rs) > 0.8;  // 0.4 : 0.1 (Particle.cpp:682-701)
+    const double v = curand_uniform_double(&rs);  // 0.4 : 0.1 : 0.1 (Particle.cpp:682-701)
+    const int kind = v <= 4.0 / 6.0 ? 0 : (v <= 5.0 / 6.0 ? 1 : 2);
+    const bool subtree = kind == 1;
     int x = root;
-    for (int tries = 0; tries < 64 && x == root; ++tries)  // uniform non-root node
-        x = min(N - 1, (int)((1.0 - curand_uniform_double(&rs)) * N));
-    if (x == root) x = root == 0 ? 1 : 0;
-    const double sc = exp((subtree ? a.subtree_delta : a.scale_delta) * (curand_uniform_double(&rs) - 0.5));
+    for (int tries = 0; tries < 64 && (x == root || (kind == 2 && x < T)); ++tries)
+        x = min(N - 1, (int)((1.0 - curand_uniform_double(&rs)) * N));  // uniform node
+    if (x == root || (kind == 2 && x < T))  // (after 64 misses) the first admissible node
+        for (int n = (kind == 2 ? T : 0); n < N; ++n)
+            if (n != root) { x = n; break; }
+    if (kind == 2) {
+        // NNIMove (Tree.cpp:625-671): one child n1 of x trades places with x's
+        // sibling n2; branch lengths stay with their nodes, so no P changes.
+        const int pa = par[x];
+        const int s1 = curand_uniform_double(&rs) <= 0.5 ? 0 : 1;
+        const int n1 = kids[2 * x + s1];
+        const int s2 = kids[2 * pa] == x ? 1 : 0;
+        const int n2 = kids[2 * pa + s2];
+        par[n1] = pa;
+        par[n2] = x;
+        kids[2 * pa + s2] = n1;
+        kids[2 * x + s1] = n2;
+        int32_t* u6 = a.nni + (size_t)i * 6;
+        u6[0] = x; u6[1] = pa; u6[2] = n1; u6[3] = n2; u6[4] = s1; u6[5] = s2;
+        a.nundo[i] = 0;
+        a.kind[i] = 2;
+        dirty[x] |= 2;
+        for (int y = pa, g = 0; y >= 0 && g < N; y = par[y], ++g) dirty[y] |= 2;
+    }
+    const double sc = kind == 2 ? 1.0
+                                : exp((subtree ? a.subtree_delta : a.scale_delta) * (curand_uniform_double(&rs) - 0.5));
     // Scale x's branch, or every branch of x's subtree (walk order: pre-order
     // with the second child first; reversed it is a post-order).
     int nch = 0, top = 0;
-    stk[top++] = x;
+    if (kind != 2) stk[top++] = x;
     while (top > 0) {  // every node is pushed once: top <= N, nch <= N
         const int n = stk[--top];
         un[nch] = n;
@@ -120,12 +148,14 @@ __global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
             stk[top++] = kids[2 * n + 1];
         }
     }
-    a.nundo[i] = nch;
-    a.kind[i] = subtree ? 1 : 0;
-    if (subtree)
-        for (int q = 0; q < nch; ++q)
-            if (un[q] >= T) dirty[un[q]] |= 2;
-    for (int y = par[x], g = 0; y >= 0 && g < N; y = par[y], ++g) dirty[y] |= 2;
+    if (kind != 2) {
+        a.nundo[i] = nch;
+        a.kind[i] = subtree ? 1 : 0;
+        if (subtree)
+            for (int q = 0; q < nch; ++q)
+                if (un[q] >= T) dirty[un[q]] |= 2;
+        for (int y = par[x], g = 0; y >= 0 && g < N; y = par[y], ++g) dirty[y] |= 2;
+    }
     const uint8_t* kc = a.clws + (size_t)i * N;
     const uint8_t* kp = a.pws + (size_t)i * N;
     uint8_t* cc = a.cur_clws + (size_t)i * N;
@@ -150,6 +180,7 @@ __global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
     if (subtree)
         for (int q = nch - 1; q >= 0; --q)
             if (un[q] >= T) emit(un[q]);
+    if (kind == 2) emit(x);  // x's new children are clean; then its ancestors
     for (int y = par[x], g = 0; y >= 0 && g < N; y = par[y], ++g) emit(y);
     PJob* pj = a.pjobs + (size_t)i * N;
     for (int q = 0; q < nch; ++q) pj[q] = PJob{a.first + i, un[q], cp[un[q]], 0, br[un[q]]};
@@ -192,6 +223,15 @@ __global__ void __launch_bounds__(kDmThreads) dm_mh_kernel(DmArgs a) {
             if (dirty[n] & 1) kp[n] = a.cur_pws[(size_t)i * N + n];
         }
         atomicAdd(&a.stats[2 * kind + 1], 1ull);
+    } else if (kind == 2) {
+        a.lnl[p] = a.lnl_old[p];
+        const int32_t* u6 = a.nni + (size_t)i * 6;
+        int32_t* par = a.parent + (size_t)i * N;
+        int32_t* kids = a.kids + (size_t)i * 2 * N;
+        par[u6[2]] = u6[0];
+        par[u6[3]] = u6[1];
+        kids[2 * u6[1] + u6[5]] = u6[3];
+        kids[2 * u6[0] + u6[4]] = u6[2];
     } else {
         a.lnl[p] = a.lnl_old[p];
         double* br = a.branch + (size_t)i * N;
@@ -265,19 +305,21 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
     size_t off = 0;
     auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 255) & ~size_t(255); return o; };
     const size_t cN = (size_t)count * N;
-    const size_t o_par = take(cN * 4), o_kids = take(2 * cN * 4), o_br = take(cN * 8), o_clws = take(cN),
+    const size_t o_par = take(cN * 4), o_kids = take(2 * cN * 4), o_nni = take((size_t)count * 6 * 4),
+                 o_br = take(cN * 8), o_clws = take(cN),
                  o_pws = take(cN), o_cc = take(cN), o_cp = take(cN), o_dirty = take(cN), o_stack = take(cN * 4),
                  o_un = take(cN * 4), o_ul = take(cN * 8), o_nundo = take((size_t)count * 4),
                  o_kind = take((size_t)count * 4), o_extra = take((size_t)count * 8),
                  o_hdr0 = take((size_t)count * sizeof(PartHdr)), o_hdr = take((size_t)count * sizeof(PartHdr)),
                  o_nodes = take((size_t)count * NI * sizeof(NodeJob)), o_pj = take(cN * sizeof(PJob)),
                  o_mj = take((size_t)count * d.Kmax * nchunk * sizeof(PmJob)),
-                 o_rng = take((size_t)count * sizeof(curandStatePhilox4_32_10_t)), o_stats = take(4 * 8);
+                 o_rng = take((size_t)count * sizeof(curandStatePhilox4_32_10_t)), o_stats = take(6 * 8);
     unsigned char* buf = nullptr;
     cudaError_t e = cudaMalloc(&buf, off);
     if (e != cudaSuccess) return dm_fail(SMCCAT_ENOMEM, "device-move buffers: " + std::string(cudaGetErrorString(e)));
     a.parent = reinterpret_cast<int32_t*>(buf + o_par);
     a.kids = reinterpret_cast<int32_t*>(buf + o_kids);
+    a.nni = reinterpret_cast<int32_t*>(buf + o_nni);
     a.branch = reinterpret_cast<double*>(buf + o_br);
     a.clws = buf + o_clws;
     a.pws = buf + o_pws;
@@ -320,7 +362,7 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
     DM_CK(cudaMemcpyAsync(a.clws, clws.data(), cN, cudaMemcpyHostToDevice, st));
     DM_CK(cudaMemcpyAsync(a.pws, pws.data(), cN, cudaMemcpyHostToDevice, st));
     DM_CK(cudaMemcpyAsync(buf + o_hdr0, hdr0.data(), (size_t)count * sizeof(PartHdr), cudaMemcpyHostToDevice, st));
-    DM_CK(cudaMemsetAsync(a.stats, 0, 4 * 8, st));
+    DM_CK(cudaMemsetAsync(a.stats, 0, 6 * 8, st));
     const int grid = (count + kDmThreads - 1) / kDmThreads;
     dm_init_kernel<<<grid, kDmThreads, 0, st>>>(a.rng, count, first, (unsigned long long)seed);
     DM_CK(cudaGetLastError());
@@ -356,11 +398,12 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
             for (int k = 0; k < steps; ++k) DM_CK(step());
         }
     }
-    unsigned long long h_stats[4];
+    unsigned long long h_stats[6];
     int status = 0;
     DM_CK(cudaMemcpyAsync(h_stats, a.stats, sizeof(h_stats), cudaMemcpyDeviceToHost, st));
     DM_CK(cudaMemcpyAsync(&status, v.status, sizeof(int), cudaMemcpyDeviceToHost, st));
     DM_CK(cudaMemcpyAsync(br.data(), a.branch, cN * 8, cudaMemcpyDeviceToHost, st));
+    DM_CK(cudaMemcpyAsync(par.data(), a.parent, cN * 4, cudaMemcpyDeviceToHost, st));
     DM_CK(cudaMemcpyAsync(clws.data(), a.clws, cN, cudaMemcpyDeviceToHost, st));
     DM_CK(cudaMemcpyAsync(pws.data(), a.pws, cN, cudaMemcpyDeviceToHost, st));
     DM_CK(cudaStreamSynchronize(st));
@@ -370,17 +413,25 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
                       status & 2 ? "a pruning warp gave up waiting for its transition matrices"
                                  : "a log-likelihood came out NaN");
     }
-    // The host mirrors take the final committed state back.
+    // The host mirrors take the final committed state back; children and
+    // post-order are regenerated from the parent tables.
     for (int i = 0; i < count; ++i) {
+        Mirror tree;
+        if (!rebuild_tree(d.T, &par[(size_t)i * N], &tree))
+            return finish(SMCCAT_ENUMERIC, "device tree moves left an invalid tree");
         Slot& s = slot_mut(c, first + i);
         for (Mirror* m : {&s.cur, &s.old}) {
+            m->parent = tree.parent;
+            m->kids = tree.kids;
+            m->post = tree.post;
+            m->root = tree.root;
             std::copy(&br[(size_t)i * N], &br[(size_t)i * N] + N, m->branch.begin());
             std::copy(&clws[(size_t)i * N], &clws[(size_t)i * N] + N, m->clws.begin());
             std::copy(&pws[(size_t)i * N], &pws[(size_t)i * N] + N, m->pws.begin());
         }
     }
     if (stats)
-        for (int k = 0; k < 4; ++k) stats[k] = (int64_t)h_stats[k];
+        for (int k = 0; k < 6; ++k) stats[k] = (int64_t)h_stats[k];
     return finish(SMCCAT_OK, "");
 #undef DM_CK
 }

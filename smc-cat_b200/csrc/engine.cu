@@ -813,6 +813,7 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
 
 const Slot& smccat::slot_of(const smccat_ctx* c, int p) { return c->slots[p]; }
 Slot& smccat::slot_mut(smccat_ctx* c, int p) { return c->slots[p]; }
+bool smccat::rebuild_tree(int T, const int32_t* parent, Mirror* m) { return build_tree(T, parent, m); }
 
 int smccat::device_view(smccat_ctx* c, int first, int count, DeviceView* v) {
     if (c->tiles_dirty) return fail(SMCCAT_ESTATE, "refresh the particles first");

@@ -91,5 +91,8 @@ struct DeviceView {
 int device_view(smccat_ctx* c, int first, int count, DeviceView* v);
 // Mutable host mirror of one slot (the device-side moves write their results back).
 Slot& slot_mut(smccat_ctx* c, int p);
+// Children, internal post-order and root of a mirror from a parent array;
+// false if it is not a rooted binary tree over 2T-1 nodes.
+bool rebuild_tree(int T, const int32_t* parent, Mirror* m);
 
 }  // namespace smccat

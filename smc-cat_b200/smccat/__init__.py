@@ -369,14 +369,15 @@ class Engine:
         return bits[:m], prob[:m]
 
     def branch_sweep(self, steps, temperature, seed, use_graph=True, first=0, count=None) -> dict:
-        """Branch-length MCMC steps entirely on the device (one CUDA graph)."""
+        """Branch-length and NNI MCMC steps entirely on the device (one CUDA graph)."""
         count = self.P - first if count is None else count
-        st = np.zeros(4, dtype=np.int64)
+        st = np.zeros(6, dtype=np.int64)
         _check(lib().smccat_branch_sweep(self._h, int(first), int(count), int(steps),
                                          float(temperature), int(seed), 1 if use_graph else 0,
                                          st.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
         return {"branch_proposed": int(st[0]), "branch_accepted": int(st[1]),
-                "subtree_proposed": int(st[2]), "subtree_accepted": int(st[3])}
+                "subtree_proposed": int(st[2]), "subtree_accepted": int(st[3]),
+                "nni_proposed": int(st[4]), "nni_accepted": int(st[5])}
 
     def rate_cholesky(self) -> np.ndarray:
         out = np.zeros((190, 190))

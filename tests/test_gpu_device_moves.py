@@ -1,7 +1,7 @@
-"""Branch-length rejuvenation with proposals, plans and accept/reject on the
-device (smccat_branch_sweep), captured as one CUDA graph: final likelihoods
-exact against the oracle, graph and eager launches identical, host path
-consistent afterwards."""
+"""Tree rejuvenation (branch scale, subtree scale, NNI) with proposals, plans
+and accept/reject on the device (smccat_branch_sweep), captured as one CUDA
+graph: final likelihoods exact against the oracle, graph and eager launches
+identical, host path consistent afterwards."""
 import numpy as np
 import pytest
 
@@ -45,11 +45,12 @@ def test_branch_sweep_keeps_exact_likelihoods(cfg):
     before = eng.get_particles()
     stats = eng.branch_sweep(steps=25, temperature=0.7, seed=5)
     n = cfg.particles
-    assert stats["branch_proposed"] + stats["subtree_proposed"] == 25 * n
+    assert stats["branch_proposed"] + stats["subtree_proposed"] + stats["nni_proposed"] == 25 * n
     assert 0 < stats["branch_accepted"] <= stats["branch_proposed"]
     assert stats["subtree_accepted"] <= stats["subtree_proposed"]
+    assert stats["nni_accepted"] <= stats["nni_proposed"]
+    assert stats["nni_proposed"] > 0
     fin = eng.get_particles()
-    np.testing.assert_array_equal(fin["parent"], before["parent"])  # topology untouched
     assert np.any(fin["branch"] != before["branch"])
     got = eng.lnl()
     for i in range(n):
@@ -63,6 +64,45 @@ def test_branch_sweep_keeps_exact_likelihoods(cfg):
     eng.close()
 
 
+def _splits(parent, T):
+    """Tip sets below every internal node, as frozensets."""
+    N = len(parent)
+    below = [{n} if n < T else set() for n in range(N)]
+    changed = True
+    while changed:
+        changed = False
+        for n in range(N):
+            p = parent[n]
+            if p >= 0 and not below[n] <= below[p]:
+                below[p] |= below[n]
+                changed = True
+    return {frozenset(b) for n, b in enumerate(below) if n >= T}
+
+
+@pytest.mark.parametrize("cfg", CFGS, ids=lambda c: c.name)
+def test_nni_changes_topology_exactly(cfg):
+    # At temperature 0 the target is the prior alone: every NNI (prior and
+    # Hastings terms both zero) is accepted, so topologies must move.
+    eng, codes, st = engine(cfg, seed=cfg.seed + 1)
+    before = eng.get_particles()
+    stats = eng.branch_sweep(steps=30, temperature=0.0, seed=12)
+    assert stats["nni_proposed"] > 0
+    assert stats["nni_accepted"] == stats["nni_proposed"]
+    fin = eng.get_particles()
+    moved = 0
+    for i in range(cfg.particles):
+        assert (fin["parent"][i] < 0).sum() == 1
+        moved += _splits(fin["parent"][i], cfg.T) != _splits(before["parent"][i], cfg.T)
+    assert moved > 0
+    got = eng.lnl()
+    for i in range(cfg.particles):
+        assert got[i] == pytest.approx(oracle_lnl(codes, cfg, fin, i), rel=1e-9)
+    # a full refresh of the synchronised trees reproduces the incremental values
+    eng.refresh(full=True)
+    np.testing.assert_allclose(eng.lnl(), got, rtol=1e-12, atol=0)
+    eng.close()
+
+
 def test_graph_and_eager_launches_agree():
     cfg = CFGS[1]
     a, _, _ = engine(cfg)
@@ -71,6 +111,7 @@ def test_graph_and_eager_launches_agree():
     sb = b.branch_sweep(steps=10, temperature=1.0, seed=77, use_graph=False)
     assert sa == sb
     np.testing.assert_array_equal(a.get_particles()["branch"], b.get_particles()["branch"])
+    np.testing.assert_array_equal(a.get_particles()["parent"], b.get_particles()["parent"])
     np.testing.assert_array_equal(a.lnl(), b.lnl())
     a.close()
     b.close()
