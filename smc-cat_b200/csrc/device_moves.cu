@@ -291,7 +291,7 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
         for (int r = 0; r < kMaxRates; ++r) h.rates[r] = m.rates[r];
     }
 
-    // One allocation carved into the argument arrays.
+    // One context-owned device buffer carved into the argument arrays.
     DmArgs a{};
     a.d = d;
     a.first = first;
@@ -314,9 +314,8 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
                  o_nodes = take((size_t)count * NI * sizeof(NodeJob)), o_pj = take(cN * sizeof(PJob)),
                  o_mj = take((size_t)count * d.Kmax * nchunk * sizeof(PmJob)),
                  o_rng = take((size_t)count * sizeof(curandStatePhilox4_32_10_t)), o_stats = take(6 * 8);
-    unsigned char* buf = nullptr;
-    cudaError_t e = cudaMalloc(&buf, off);
-    if (e != cudaSuccess) return dm_fail(SMCCAT_ENOMEM, "device-move buffers: " + std::string(cudaGetErrorString(e)));
+    unsigned char* buf = moves_buffer(c, off);
+    if (!buf) return dm_fail(SMCCAT_ENOMEM, "device-move buffers: out of device memory");
     a.parent = reinterpret_cast<int32_t*>(buf + o_par);
     a.kids = reinterpret_cast<int32_t*>(buf + o_kids);
     a.nni = reinterpret_cast<int32_t*>(buf + o_nni);
@@ -347,7 +346,6 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         cudaStreamSynchronize(st);
-        cudaFree(buf);
         if (code) set_last_error(msg);
         return code;
     };

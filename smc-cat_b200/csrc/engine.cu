@@ -76,6 +76,8 @@ struct smccat_ctx {
     double* d_site_lnl = nullptr;
     int* d_status = nullptr;
     char* d_plan = nullptr;
+    unsigned char* d_moves = nullptr;  // device tree-move buffers, grow-only
+    size_t moves_cap = 0;
 
     char* h_plan = nullptr;     // pinned
     uint8_t* h_sws = nullptr;   // pinned mirror of d_sws
@@ -287,7 +289,7 @@ int smccat_destroy(smccat_ctx* c) {
     if (c->st) cudaStreamSynchronize(c->st);
     void* dptrs[] = {c->d_codes, c->d_isinv, c->d_invchar, c->d_perm, c->d_tiles, c->d_tile_off,
                      c->d_CL, c->d_LSC, c->d_Pm, c->d_spec, c->d_sws, c->d_partial, c->d_lnl,
-                     c->d_lnl_old, c->d_site_lnl, c->d_status, c->d_plan, c->d_wt};
+                     c->d_lnl_old, c->d_site_lnl, c->d_status, c->d_plan, c->d_wt, c->d_moves};
     for (void* p : dptrs) if (p) cudaFree(p);
     if (c->h_plan) cudaFreeHost(c->h_plan);
     if (c->h_sws) cudaFreeHost(c->h_sws);
@@ -814,6 +816,18 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
 const Slot& smccat::slot_of(const smccat_ctx* c, int p) { return c->slots[p]; }
 Slot& smccat::slot_mut(smccat_ctx* c, int p) { return c->slots[p]; }
 bool smccat::rebuild_tree(int T, const int32_t* parent, Mirror* m) { return build_tree(T, parent, m); }
+
+unsigned char* smccat::moves_buffer(smccat_ctx* c, size_t bytes) {
+    if (bytes > c->moves_cap) {
+        cudaStreamSynchronize(c->st);
+        if (c->d_moves) cudaFree(c->d_moves);
+        c->d_moves = nullptr;
+        c->moves_cap = 0;
+        if (cudaMalloc((void**)&c->d_moves, bytes) != cudaSuccess) return nullptr;
+        c->moves_cap = bytes;
+    }
+    return c->d_moves;
+}
 
 int smccat::device_view(smccat_ctx* c, int first, int count, DeviceView* v) {
     if (c->tiles_dirty) return fail(SMCCAT_ESTATE, "refresh the particles first");

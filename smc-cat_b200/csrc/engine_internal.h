@@ -94,5 +94,8 @@ Slot& slot_mut(smccat_ctx* c, int p);
 // Children, internal post-order and root of a mirror from a parent array;
 // false if it is not a rooted binary tree over 2T-1 nodes.
 bool rebuild_tree(int T, const int32_t* parent, Mirror* m);
+// Device buffer of at least `bytes` owned by the context (kept between calls,
+// reallocated only to grow; freed with the context). nullptr if out of memory.
+unsigned char* moves_buffer(smccat_ctx* c, size_t bytes);
 
 }  // namespace smccat
