@@ -569,6 +569,9 @@ def main():
     if args.sweeps > 0:
         load()
         eng.refresh(full=True)
+        # Split posteriors of the population for adaptive NNI (main.cpp:203),
+        # installed for this and the device sweep below.
+        eng.compute_split_posteriors()
         eng.rejuvenate(iterations=cfg.iterations, temperature=args.sweep_temp, seed=999 + rank)
         barrier()
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -580,12 +583,12 @@ def main():
         s1.synchronize()
         barrier()
         ms_sweep = s0.elapsed_time(s1)
-    # ---- branch-length / NNI sweep with everything on the device (one CUDA graph) ----
+    # ---- tree-move sweep with everything on the device (one CUDA graph) ----
     dev_sweep, ms_dev = None, 0.0
     if args.sweeps > 0 and args.branch_steps > 0:
         load()
         eng.refresh(full=True)
-        eng.branch_sweep(steps=4, temperature=args.sweep_temp, seed=5 + rank)
+        eng.tree_sweep(steps=4, temperature=args.sweep_temp, seed=5 + rank)
         # Three sweeps from the same state; the median is reported (a single
         # call includes graph capture and instantiation, which can stall).
         reps = []
@@ -595,14 +598,14 @@ def main():
             barrier()
             d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             d0.record(stream)
-            bst = eng.branch_sweep(steps=args.branch_steps, temperature=args.sweep_temp,
+            bst = eng.tree_sweep(steps=args.branch_steps, temperature=args.sweep_temp,
                                    seed=6 + rank)
             d1.record(stream)
             d1.synchronize()
             barrier()
             reps.append(d0.elapsed_time(d1))
         ms_dev = float(np.median(reps))
-        dev_sweep = {"what": "scaleBranch / scaleSubtree / NNI MH steps (4 : 1 : 1) on every particle, proposals, plans "
+        dev_sweep = {"what": "treeMove MH steps (NNI, adaptive NNI, SPR, branch, subtree scale: 0.1 / 0.3 / 0.1 / 0.4 / 0.1) on every particle, proposals, plans "
                              "and accept/reject on the device, captured as one CUDA graph "
                              "(upload, capture and sync-back included); median of 3 sweeps",
                      "steps": args.branch_steps, "ms_per_sweep_each": reps, **bst}
@@ -751,7 +754,7 @@ def main():
             "gpu_launches": sum(prof["launches"].values()),
             "mixed_precision": mixed,
             "site_patterns": pat,
-            "device_branch_sweep": dev_sweep,
+            "device_tree_sweep": dev_sweep,
             "sweeps_per_s": (args.sweeps / (ms_sweep * 1e-3)) if args.sweeps > 0 else None,
             "sweep": None if sweep_stats is None else {
                 "definition": f"Mcmc::operator() with {cfg.iterations} iterations on all {n} "

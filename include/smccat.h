@@ -286,20 +286,21 @@ int smccat_resample_tune(smccat_ctx* ctx, int32_t first, int32_t count, const do
                          double u, int32_t copy, int32_t* ancestors);
 
 /* Tree rejuvenation with everything on the device: `steps` lockstep
- * Metropolis-Hastings steps of Tree::scaleBranchMove, Tree::scaleSubtreeMove
- * and Tree::NNIMove (Tree.cpp:553-671, in their 0.4 : 0.1 : 0.1 proportion of
- * Particle::treeMove, Particle.cpp:682-701) on every particle of
- * [first, first+count), at `temperature`, with the tuned scale_delta /
- * subtree_scale_delta. Each step's proposal, dirty-node plan, transition
- * matrices, pruning, reduction and accept/reject run as device kernels with
- * fixed launch shapes; with use_graph != 0 the whole sweep is captured as one
- * CUDA graph and launched once. Draws come from a Philox stream per particle
- * seeded by `seed`. Afterwards the host state holds the final trees and branch
- * lengths (adaptive NNI and SPR stay with smccat_rejuvenate). Needs refreshed,
- * committed particles. stats (may be NULL, else 6 entries): proposed /
- * accepted scaleBranch, scaleSubtree, NNI. */
-int smccat_branch_sweep(smccat_ctx* ctx, int32_t first, int32_t count, int32_t steps,
-                        double temperature, uint64_t seed, int32_t use_graph, int64_t* stats);
+ * Metropolis-Hastings steps of Particle::treeMove (Particle.cpp:677-701: NNI
+ * 0.1, adaptive NNI 0.3, SPR 0.1, scaleBranch 0.4, scaleSubtree 0.1;
+ * Tree.cpp:553-812) on every particle of [first, first+count), at
+ * `temperature`, with the tuned scale_delta / subtree_scale_delta /
+ * adaptive_nni_epsilon and the installed split posteriors. Each step's
+ * proposal, dirty-node plan, transition matrices, pruning, reduction and
+ * accept/reject run as device kernels with fixed launch shapes; with
+ * use_graph != 0 the whole sweep is captured as one CUDA graph and launched
+ * once. Draws come from a Philox stream per particle seeded by `seed`.
+ * Afterwards the host state holds the final trees and branch lengths. Needs
+ * refreshed, committed particles. stats (may be NULL, else 10 entries):
+ * stats[2k] proposed and stats[2k+1] accepted moves of kind k =
+ * SMCCAT_MOVE_ADAPTIVE_NNI .. SMCCAT_MOVE_SCALE_SUBTREE. */
+int smccat_tree_sweep(smccat_ctx* ctx, int32_t first, int32_t count, int32_t steps,
+                      double temperature, uint64_t seed, int32_t use_graph, int64_t* stats);
 
 /* Particle::lnPrior (Particle.cpp:484-517) of the current states. */
 int smccat_ln_prior(smccat_ctx* ctx, int32_t first, int32_t count, double* out);

@@ -1,33 +1,36 @@
 // Tree moves on the device, a whole sweep captured as one CUDA graph.
 //
 // The host MCMC driver (mcmc.cu) proposes every move on host mirrors and packs
-// each step's plan on the host. Here three moves of the reference's tree-move
-// mixture -- Tree::scaleBranchMove, Tree::scaleSubtreeMove (Tree.cpp:553-612)
-// and Tree::NNIMove (Tree.cpp:625-671), 0.4, 0.1 and 0.1 of
-// Particle::treeMove (Particle.cpp:682-701), so 4 : 1 : 1 here -- run for
+// each step's plan on the host. Here the reference's whole tree-move mixture,
+// Particle::treeMove (Particle.cpp:677-701) -- NNI 0.1, adaptive NNI 0.3,
+// SPR 0.1, branch scale 0.4, subtree scale 0.1 (Tree.cpp:553-812) -- runs for
 // every particle of a range in lockstep with nothing on the host between steps:
 //
-//   dm_propose_kernel   one thread per particle: Philox draws, the array edit of
-//                       the flattened tree (branch lengths, or for NNI the
-//                       swap of one child of x with x's sibling in the parent
-//                       and child tables), the dirty sets (scaled nodes'
-//                       transition matrices; the subtree's internal partials,
-//                       or x for NNI, and every ancestor), the plan in
-//                       post-order with the next workspaces, the tree-length
-//                       prior change and the log Hastings ratio;
+//   dm_propose_kernel   one thread per particle: Philox draws, the edit of the
+//                       flattened tree (branch lengths; or parent / child
+//                       table entries, logged for undo), the dirty sets, the
+//                       plan in post-order with the next workspaces, the
+//                       tree-length prior change and the log Hastings ratio.
+//                       Adaptive NNI weighs nodes by their split's posterior,
+//                       looked up by binary search in a sorted split table;
 //   pmat_kernel, prune_kernel, reduce_kernel
 //                       the engine's kernels on that device-built plan, with
 //                       launch shapes fixed by the range (empty job slots exit);
 //   dm_mh_kernel        one thread per particle: Metropolis-Hastings on
 //                       temperature * lnL + lnPrior + log Hastings (Mcmc.cpp:57-60);
 //                       accept commits the new workspaces, reject restores the
-//                       branch lengths or the parent / child tables (the dirty
+//                       branch lengths or replays the table undo log (the dirty
 //                       work sits in the other workspace, as on the host path).
 //
 // A sweep of B steps is B repetitions of this fixed sequence, captured into a
 // CUDA graph and launched once. At the end the host mirrors take the final
 // trees (children and post-order regenerated from the parent tables), branch
 // lengths and committed workspaces back.
+//
+// Partials invalidated by a topology move: the moved node and its ancestors,
+// and for SPR also the old parent's ancestors. (The reference's SPRMove marks
+// only the new path, Tree.cpp:803-807, leaving the old parent's partials stale
+// until the next full refresh; the host path and this one mark both.)
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
 #include <math.h>
@@ -45,25 +48,37 @@ namespace smccat {
 namespace {
 
 constexpr int kDmThreads = 64;
+constexpr int kUndo = 8;  // table edits of one move (SPR: 6, NNI: 4)
+
+// Move kinds, numbered like SMCCAT_MOVE_*.
+constexpr int kAnni = 0, kNni = 1, kSpr = 2, kBranch = 3, kSubtree = 4;
 
 struct DmArgs {
     Dims d;
     int first, count, nchunk;
     int32_t* parent;     // [count][N]
     int32_t* kids;       // [count][2N]
-    int32_t* nni;        // [count][6] x, a, n1, n2 and their child-slot indices
+    int32_t* ulog;       // [count][2 kUndo] (table index, old value); index >= N is kids[index - N]
+    int32_t* nlog;       // [count]
     double* branch;      // [count][N]
     uint8_t* clws;       // [count][N] committed partial workspace of each node
     uint8_t* pws;        // [count][N] committed transition-matrix workspace
     uint8_t* cur_clws;   // [count][N] workspaces of this step's proposal
     uint8_t* cur_pws;
-    uint8_t* dirty;      // [count][N] bit 0: P, bit 1: partial
-    int32_t* stack;      // [count][N] subtree walk
+    uint8_t* dirty;      // [count][N] bit 0: P, bit 1: partial, bit 2: on the first path
+    int32_t* stack;      // [count][N] walks
+    int32_t* order;      // [count][N] dirty internal nodes, children first
     int32_t* undo_node;  // [count][N] scaled nodes, walk order
     double* undo_len;    // [count][N] their previous lengths
     int32_t* nundo;      // [count]
-    int32_t* kind;       // [count] 0 scaleBranch, 1 scaleSubtree, 2 NNI
+    int32_t* kind;       // [count] SMCCAT_MOVE_* of this step's move
     double* extra;       // [count] lnPrior change + log Hastings ratio
+    uint64_t* clade;     // [count][N][2] taxa below each node (adaptive NNI)
+    double* wnode;       // [count][N] adaptive-NNI node weights
+    const uint64_t* skeys;  // [nsplit][2] canonical splits, sorted
+    const double* sprob;    // [nsplit]
+    int nsplit;
+    bool use_splits;     // T <= 128: splits fit two words
     const PartHdr* hdr0; // [count] root, classes, pinv, rates
     PartHdr* hdr;        // [count] this step's
     NodeJob* nodes;      // [count][NI]
@@ -72,13 +87,41 @@ struct DmArgs {
     curandStatePhilox4_32_10_t* rng;  // [count]
     double* lnl;         // engine arrays, [max_particles]
     double* lnl_old;
-    unsigned long long* stats;  // proposed / accepted, per kind (6)
-    double scale_delta, subtree_delta, temp;
+    unsigned long long* stats;  // proposed / accepted per move kind (10)
+    double scale_delta, subtree_delta, anni_eps, temp;
 };
 
 __global__ void dm_init_kernel(curandStatePhilox4_32_10_t* rng, int count, int first, unsigned long long seed) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < count) curand_init(seed, (unsigned long long)(first + i), 0ull, &rng[i]);
+}
+
+// Posterior of a canonical split, or -1 when the table does not hold it.
+__device__ double split_lookup(const DmArgs& a, uint64_t w0, uint64_t w1) {
+    int lo = 0, hi = a.nsplit;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const uint64_t k0 = a.skeys[2 * mid], k1 = a.skeys[2 * mid + 1];
+        if (k0 < w0 || (k0 == w0 && k1 < w1)) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo < a.nsplit && a.skeys[2 * lo] == w0 && a.skeys[2 * lo + 1] == w1) return a.sprob[lo];
+    return -1.0;
+}
+
+// Adaptive-NNI weight of a node whose clade is (c0, c1) (Tree.cpp:676-694):
+// epsilon + 1 - posterior of its split, epsilon + 1 when the split is absent
+// or trivial. Splits are canonicalised to contain taxon 0.
+__device__ double anni_weight(const DmArgs& a, uint64_t c0, uint64_t c1) {
+    double v = a.anni_eps;
+    if (!a.use_splits) return v + 1.0;
+    const int T = a.d.T;
+    const uint64_t f0 = T >= 64 ? ~0ull : (1ull << T) - 1;
+    const uint64_t f1 = T <= 64 ? 0ull : (T >= 128 ? ~0ull : (1ull << (T - 64)) - 1);
+    if (!(c0 & 1ull)) { c0 = ~c0 & f0; c1 = ~c1 & f1; }
+    const int cnt = __popcll(c0) + __popcll(c1);
+    const double pr = (cnt == 1 || cnt == T - 1) ? -1.0 : split_lookup(a, c0, c1);
+    return v + (pr >= 0.0 ? 1.0 - pr : 1.0);
 }
 
 __global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
@@ -91,71 +134,190 @@ __global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
     double* br = a.branch + (size_t)i * N;
     uint8_t* dirty = a.dirty + (size_t)i * N;
     int32_t* stk = a.stack + (size_t)i * N;
+    int32_t* ord = a.order + (size_t)i * N;
     int32_t* un = a.undo_node + (size_t)i * N;
     double* ul = a.undo_len + (size_t)i * N;
+    int32_t* lg = a.ulog + (size_t)i * 2 * kUndo;
     const PartHdr h0 = a.hdr0[i];
     const int root = h0.root;
     curandStatePhilox4_32_10_t rs = a.rng[i];
+    auto unif = [&]() { return 1.0 - curand_uniform_double(&rs); };  // [0, 1)
+    auto uniform_node = [&]() { return min(N - 1, (int)(unif() * N)); };
+    // A uniform node other than the root (internal only if `internal`); after
+    // 64 misses the first admissible id (probability below 1e-12 for T >= 3).
+    auto pick = [&](bool internal) {
+        int x = root;
+        for (int t = 0; t < 64 && (x == root || (internal && x < T)); ++t) x = uniform_node();
+        if (x == root || (internal && x < T))
+            for (int n = internal ? T : 0; n < N; ++n)
+                if (n != root) { x = n; break; }
+        return x;
+    };
+    auto in_subtree = [&](int y, int r) {  // Tree.hpp:29-34
+        for (int g = 0; y >= 0 && g <= N; y = par[y], ++g)
+            if (y == r) return true;
+        return false;
+    };
+    int nlog = 0;
+    auto set_par = [&](int n, int v) {
+        lg[2 * nlog] = n; lg[2 * nlog + 1] = par[n]; ++nlog;
+        par[n] = v;
+    };
+    auto set_kid = [&](int k, int v) {
+        lg[2 * nlog] = N + k; lg[2 * nlog + 1] = kids[k]; ++nlog;
+        kids[k] = v;
+    };
+    int nord = 0;
+    // Dirty partials on two root paths, recorded children first: the path of
+    // `b` up to where it meets the path of `pa`, then the path of `pa`.
+    auto mark_paths = [&](int pa, int b) {
+        for (int y = pa, g = 0; y >= 0 && g < N; y = par[y], ++g) dirty[y] |= 2 | 4;
+        for (int y = b, g = 0; y >= 0 && g < N && !(dirty[y] & 4); y = par[y], ++g) {
+            dirty[y] |= 2;
+            if (nord < N) ord[nord++] = y;
+        }
+        for (int y = pa, g = 0; y >= 0 && g < N; y = par[y], ++g)
+            if (nord < N) ord[nord++] = y;
+    };
 
     double L0 = 0.0;
     for (int n = 0; n < N; ++n) {
         dirty[n] = 0;
         L0 += br[n];
     }
-    const double v = curand_uniform_double(&rs);  // 0.4 : 0.1 : 0.1 (Particle.cpp:682-701)
-    const int kind = v <= 4.0 / 6.0 ? 0 : (v <= 5.0 / 6.0 ? 1 : 2);
-    const bool subtree = kind == 1;
-    int x = root;
-    for (int tries = 0; tries < 64 && (x == root || (kind == 2 && x < T)); ++tries)
-        x = min(N - 1, (int)((1.0 - curand_uniform_double(&rs)) * N));  // uniform node
-    if (x == root || (kind == 2 && x < T))  // (after 64 misses) the first admissible node
-        for (int n = (kind == 2 ? T : 0); n < N; ++n)
-            if (n != root) { x = n; break; }
-    if (kind == 2) {
-        // NNIMove (Tree.cpp:625-671): one child n1 of x trades places with x's
-        // sibling n2; branch lengths stay with their nodes, so no P changes.
+    const double u = unif();  // Particle.cpp:680-701
+    const int kind = u < 0.1 ? kNni : u < 0.4 ? kAnni : u < 0.5 ? kSpr : u < 0.9 ? kBranch : kSubtree;
+    double hastings = 0.0, sc = 1.0;
+    int nch = 0;
+    if (kind == kNni || kind == kAnni) {
+        // NNIMove / adaptiveNNIMove (Tree.cpp:625-766): one child n1 of x
+        // trades places with x's sibling n2; branch lengths stay with their
+        // nodes, so no transition matrix changes.
+        int x;
+        double sel = 0.0, tot = 0.0;
+        double* wn = a.wnode + (size_t)i * N;
+        uint64_t* cl = a.clade + (size_t)i * 2 * N;
+        if (kind == kNni) {
+            x = pick(true);
+        } else {
+            if (a.use_splits) {  // clades bottom-up over a pre-order walk
+                int top = 0, cnt = 0;
+                stk[top++] = root;
+                while (top > 0 && cnt < N) {
+                    const int n = stk[--top];
+                    ord[cnt++] = n;
+                    if (n >= T && top + 2 <= N) { stk[top++] = kids[2 * n]; stk[top++] = kids[2 * n + 1]; }
+                }
+                for (int q = cnt - 1; q >= 0; --q) {
+                    const int n = ord[q];
+                    if (n < T) {
+                        cl[2 * n] = n < 64 ? 1ull << n : 0ull;
+                        cl[2 * n + 1] = n >= 64 ? 1ull << (n - 64) : 0ull;
+                    } else {
+                        const int k1 = kids[2 * n], k2 = kids[2 * n + 1];
+                        cl[2 * n] = cl[2 * k1] | cl[2 * k2];
+                        cl[2 * n + 1] = cl[2 * k1 + 1] | cl[2 * k2 + 1];
+                    }
+                }
+            }
+            for (int n = T; n < N; ++n) {
+                if (n == root) continue;
+                wn[n] = a.use_splits ? anni_weight(a, cl[2 * n], cl[2 * n + 1]) : a.anni_eps + 1.0;
+                tot += wn[n];
+            }
+            const double r = unif();
+            double cum = 0.0;
+            x = -1;
+            for (int n = T; n < N; ++n) {
+                if (n == root) continue;
+                cum += wn[n] / tot;
+                x = n;
+                if (r <= cum) break;
+            }
+            sel = wn[x] / tot;
+        }
         const int pa = par[x];
-        const int s1 = curand_uniform_double(&rs) <= 0.5 ? 0 : 1;
+        const int s1 = min(1, (int)(unif() * 2));
         const int n1 = kids[2 * x + s1];
         const int s2 = kids[2 * pa] == x ? 1 : 0;
         const int n2 = kids[2 * pa + s2];
-        par[n1] = pa;
-        par[n2] = x;
-        kids[2 * pa + s2] = n1;
-        kids[2 * x + s1] = n2;
-        int32_t* u6 = a.nni + (size_t)i * 6;
-        u6[0] = x; u6[1] = pa; u6[2] = n1; u6[3] = n2; u6[4] = s1; u6[5] = s2;
-        a.nundo[i] = 0;
-        a.kind[i] = 2;
-        dirty[x] |= 2;
-        for (int y = pa, g = 0; y >= 0 && g < N; y = par[y], ++g) dirty[y] |= 2;
-    }
-    const double sc = kind == 2 ? 1.0
-                                : exp((subtree ? a.subtree_delta : a.scale_delta) * (curand_uniform_double(&rs) - 0.5));
-    // Scale x's branch, or every branch of x's subtree (walk order: pre-order
-    // with the second child first; reversed it is a post-order).
-    int nch = 0, top = 0;
-    if (kind != 2) stk[top++] = x;
-    while (top > 0) {  // every node is pushed once: top <= N, nch <= N
-        const int n = stk[--top];
-        un[nch] = n;
-        ul[nch] = br[n];
-        ++nch;
-        br[n] *= sc;
-        dirty[n] |= 1;
-        if (subtree && n >= T) {
-            stk[top++] = kids[2 * n];
-            stk[top++] = kids[2 * n + 1];
+        set_par(n1, pa);
+        set_par(n2, x);
+        set_kid(2 * pa + s2, n1);
+        set_kid(2 * x + s1, n2);
+        if (kind == kAnni) {
+            // Only x's clade changes: it loses n1's taxa and gains n2's.
+            double w2 = a.anni_eps + 1.0;
+            if (a.use_splits)
+                w2 = anni_weight(a, (cl[2 * x] & ~cl[2 * n1]) | cl[2 * n2],
+                                 (cl[2 * x + 1] & ~cl[2 * n1 + 1]) | cl[2 * n2 + 1]);
+            double tot2 = 0.0;
+            for (int n = T; n < N; ++n)
+                if (n != root) tot2 += n == x ? w2 : wn[n];
+            hastings = log(w2 / tot2) - log(sel);
         }
-    }
-    if (kind != 2) {
-        a.nundo[i] = nch;
-        a.kind[i] = subtree ? 1 : 0;
+        mark_paths(pa, x);
+    } else if (kind == kSpr) {
+        // SPRMove (Tree.cpp:768-812): prune the subtree of x's child sch (x
+        // comes with it, x's other child sib takes x's place) and regraft x
+        // on the branch above a node an outside it.
+        const int x = pick(true);
+        const int s1 = min(1, (int)(unif() * 2));
+        const int sib = kids[2 * x + 1 - s1];
+        int an = -1;
+        for (int t = 0; t < 256 && an < 0; ++t) {
+            const int c = uniform_node();
+            if (c != root && !in_subtree(c, x)) an = c;
+        }
+        if (an < 0)  // x's parent or sibling always qualifies
+            for (int n = 0; n < N && an < 0; ++n)
+                if (n != root && !in_subtree(n, x)) an = n;
+        const int gp = par[x];
+        set_kid(2 * gp + (kids[2 * gp] == x ? 0 : 1), sib);
+        set_par(sib, gp);
+        const int ap = par[an];
+        set_kid(2 * ap + (kids[2 * ap] == an ? 0 : 1), x);
+        set_par(x, ap);
+        set_kid(2 * x + 1 - s1, an);
+        set_par(an, x);
+        mark_paths(gp, x);
+    } else {
+        // scaleBranchMove / scaleSubtreeMove (Tree.cpp:553-612): x's branch,
+        // or every branch of x's subtree (walk order: pre-order with the
+        // second child first; reversed it is a post-order).
+        const bool subtree = kind == kSubtree;
+        const int x = pick(false);
+        sc = exp((subtree ? a.subtree_delta : a.scale_delta) * (unif() - 0.5));
+        int top = 0;
+        stk[top++] = x;
+        while (top > 0) {  // every node is pushed once: top <= N, nch <= N
+            const int n = stk[--top];
+            un[nch] = n;
+            ul[nch] = br[n];
+            ++nch;
+            br[n] *= sc;
+            dirty[n] |= 1;
+            if (subtree && n >= T) {
+                stk[top++] = kids[2 * n];
+                stk[top++] = kids[2 * n + 1];
+            }
+        }
         if (subtree)
-            for (int q = 0; q < nch; ++q)
-                if (un[q] >= T) dirty[un[q]] |= 2;
-        for (int y = par[x], g = 0; y >= 0 && g < N; y = par[y], ++g) dirty[y] |= 2;
+            for (int q = nch - 1; q >= 0; --q)
+                if (un[q] >= T) {
+                    dirty[un[q]] |= 2;
+                    if (nord < N) ord[nord++] = un[q];
+                }
+        for (int y = par[x], g = 0; y >= 0 && g < N; y = par[y], ++g) {
+            dirty[y] |= 2;
+            if (nord < N) ord[nord++] = y;
+        }
+        hastings = nch * log(sc);
     }
+    a.nlog[i] = nlog;
+    a.nundo[i] = nch;
+    a.kind[i] = kind;
+
     const uint8_t* kc = a.clws + (size_t)i * N;
     const uint8_t* kp = a.pws + (size_t)i * N;
     uint8_t* cc = a.cur_clws + (size_t)i * N;
@@ -164,24 +326,19 @@ __global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
         cc[n] = (dirty[n] & 2) ? 1 - kc[n] : kc[n];
         cp[n] = (dirty[n] & 1) ? 1 - kp[n] : kp[n];
     }
-    // Plan: the subtree's internal nodes in post-order, then x's ancestors up
-    // to the root; each node's children are done before it.
+    // Plan: the recorded dirty internal nodes, each after its dirty children.
     NodeJob* nj = a.nodes + (size_t)i * NI;
     int nn = 0;
-    auto emit = [&](int n) {
+    for (int q = 0; q < nord && nn < NI; ++q) {
+        const int n = ord[q];
         const int c1 = kids[2 * n], c2 = kids[2 * n + 1];
         int ws = cc[n];
         if (c1 >= T) ws |= cc[c1] << 1;
         if (c2 >= T) ws |= cc[c2] << 2;
         ws |= cp[c1] << 3;
         ws |= cp[c2] << 4;
-        if (nn < NI) nj[nn++] = NodeJob{n, c1, c2, ws};
-    };
-    if (subtree)
-        for (int q = nch - 1; q >= 0; --q)
-            if (un[q] >= T) emit(un[q]);
-    if (kind == 2) emit(x);  // x's new children are clean; then its ancestors
-    for (int y = par[x], g = 0; y >= 0 && g < N; y = par[y], ++g) emit(y);
+        nj[nn++] = NodeJob{n, c1, c2, ws};
+    }
     PJob* pj = a.pjobs + (size_t)i * N;
     for (int q = 0; q < nch; ++q) pj[q] = PJob{a.first + i, un[q], cp[un[q]], 0, br[un[q]]};
     PmJob* mj = a.mjobs + (size_t)i * d.Kmax * a.nchunk;
@@ -199,8 +356,8 @@ __global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
     double L1 = 0.0;
     for (int n = 0; n < N; ++n) L1 += br[n];
     // Tree-length prior Gamma(2T-2, scale 1/10) (Particle.cpp:484-517) and the
-    // Hastings ratio of a multiplicative scale of nch branches.
-    a.extra[i] = (N - 2) * (log(L1) - log(L0)) - (L1 - L0) / 0.1 + nch * log(sc);
+    // Hastings ratio.
+    a.extra[i] = (N - 2) * (log(L1) - log(L0)) - (L1 - L0) / 0.1 + hastings;
     a.rng[i] = rs;
 }
 
@@ -223,21 +380,20 @@ __global__ void __launch_bounds__(kDmThreads) dm_mh_kernel(DmArgs a) {
             if (dirty[n] & 1) kp[n] = a.cur_pws[(size_t)i * N + n];
         }
         atomicAdd(&a.stats[2 * kind + 1], 1ull);
-    } else if (kind == 2) {
-        a.lnl[p] = a.lnl_old[p];
-        const int32_t* u6 = a.nni + (size_t)i * 6;
-        int32_t* par = a.parent + (size_t)i * N;
-        int32_t* kids = a.kids + (size_t)i * 2 * N;
-        par[u6[2]] = u6[0];
-        par[u6[3]] = u6[1];
-        kids[2 * u6[1] + u6[5]] = u6[3];
-        kids[2 * u6[0] + u6[4]] = u6[2];
     } else {
         a.lnl[p] = a.lnl_old[p];
         double* br = a.branch + (size_t)i * N;
         const int32_t* un = a.undo_node + (size_t)i * N;
         const double* ul = a.undo_len + (size_t)i * N;
         for (int q = a.nundo[i] - 1; q >= 0; --q) br[un[q]] = ul[q];
+        int32_t* par = a.parent + (size_t)i * N;
+        int32_t* kids = a.kids + (size_t)i * 2 * N;
+        const int32_t* lg = a.ulog + (size_t)i * 2 * kUndo;
+        for (int q = a.nlog[i] - 1; q >= 0; --q) {
+            const int x = lg[2 * q];
+            if (x < N) par[x] = lg[2 * q + 1];
+            else kids[x - N] = lg[2 * q + 1];
+        }
     }
     a.rng[i] = rs;
 }
@@ -252,9 +408,9 @@ int dm_fail(int code, const std::string& msg) {
 
 using namespace smccat;
 
-extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, int32_t steps,
-                                   double temperature, uint64_t seed, int32_t use_graph,
-                                   int64_t* stats) {
+extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, int32_t steps,
+                                 double temperature, uint64_t seed, int32_t use_graph,
+                                 int64_t* stats) {
     if (!c) return dm_fail(SMCCAT_EINVAL, "null context");
     const Dims& d = dims_of(c);
     if (first < 0 || count < 1 || steps < 0) return dm_fail(SMCCAT_EINVAL, "bad range");
@@ -270,6 +426,11 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
     rc = smccat_get_tuning(c, &tn);
     if (rc) return rc;
     const int N = d.N, NI = d.NI, nchunk = (N + kPmChunk - 1) / kPmChunk;
+    const bool use_splits = d.T <= 128;
+    std::vector<uint64_t> skeys;
+    std::vector<double> sprob;
+    if (use_splits) split_table(c, &skeys, &sprob);
+    const int nsplit = (int)sprob.size();
 
     // Host images of the trees and committed workspaces.
     std::vector<int32_t> par((size_t)count * N), kids((size_t)count * 2 * N);
@@ -301,24 +462,35 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
     a.lnl_old = v.lnl_old;
     a.scale_delta = tn.scale_delta;
     a.subtree_delta = tn.subtree_scale_delta;
+    a.anni_eps = tn.adaptive_nni_epsilon;
     a.temp = temperature;
+    a.nsplit = nsplit;
+    a.use_splits = use_splits;
     size_t off = 0;
     auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 255) & ~size_t(255); return o; };
     const size_t cN = (size_t)count * N;
-    const size_t o_par = take(cN * 4), o_kids = take(2 * cN * 4), o_nni = take((size_t)count * 6 * 4),
-                 o_br = take(cN * 8), o_clws = take(cN),
+    const size_t o_par = take(cN * 4), o_kids = take(2 * cN * 4), o_log = take((size_t)count * 2 * kUndo * 4),
+                 o_nlog = take((size_t)count * 4), o_ord = take(cN * 4), o_clade = take(2 * cN * 8),
+                 o_wn = take(cN * 8), o_sk = take((size_t)std::max(nsplit, 1) * 16),
+                 o_sp = take((size_t)std::max(nsplit, 1) * 8), o_br = take(cN * 8), o_clws = take(cN),
                  o_pws = take(cN), o_cc = take(cN), o_cp = take(cN), o_dirty = take(cN), o_stack = take(cN * 4),
                  o_un = take(cN * 4), o_ul = take(cN * 8), o_nundo = take((size_t)count * 4),
                  o_kind = take((size_t)count * 4), o_extra = take((size_t)count * 8),
                  o_hdr0 = take((size_t)count * sizeof(PartHdr)), o_hdr = take((size_t)count * sizeof(PartHdr)),
                  o_nodes = take((size_t)count * NI * sizeof(NodeJob)), o_pj = take(cN * sizeof(PJob)),
                  o_mj = take((size_t)count * d.Kmax * nchunk * sizeof(PmJob)),
-                 o_rng = take((size_t)count * sizeof(curandStatePhilox4_32_10_t)), o_stats = take(6 * 8);
+                 o_rng = take((size_t)count * sizeof(curandStatePhilox4_32_10_t)), o_stats = take(10 * 8);
     unsigned char* buf = moves_buffer(c, off);
     if (!buf) return dm_fail(SMCCAT_ENOMEM, "device-move buffers: out of device memory");
     a.parent = reinterpret_cast<int32_t*>(buf + o_par);
     a.kids = reinterpret_cast<int32_t*>(buf + o_kids);
-    a.nni = reinterpret_cast<int32_t*>(buf + o_nni);
+    a.ulog = reinterpret_cast<int32_t*>(buf + o_log);
+    a.nlog = reinterpret_cast<int32_t*>(buf + o_nlog);
+    a.order = reinterpret_cast<int32_t*>(buf + o_ord);
+    a.clade = reinterpret_cast<uint64_t*>(buf + o_clade);
+    a.wnode = reinterpret_cast<double*>(buf + o_wn);
+    a.skeys = reinterpret_cast<const uint64_t*>(buf + o_sk);
+    a.sprob = reinterpret_cast<const double*>(buf + o_sp);
     a.branch = reinterpret_cast<double*>(buf + o_br);
     a.clws = buf + o_clws;
     a.pws = buf + o_pws;
@@ -360,7 +532,11 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
     DM_CK(cudaMemcpyAsync(a.clws, clws.data(), cN, cudaMemcpyHostToDevice, st));
     DM_CK(cudaMemcpyAsync(a.pws, pws.data(), cN, cudaMemcpyHostToDevice, st));
     DM_CK(cudaMemcpyAsync(buf + o_hdr0, hdr0.data(), (size_t)count * sizeof(PartHdr), cudaMemcpyHostToDevice, st));
-    DM_CK(cudaMemsetAsync(a.stats, 0, 6 * 8, st));
+    DM_CK(cudaMemsetAsync(a.stats, 0, 10 * 8, st));
+    if (nsplit > 0) {
+        DM_CK(cudaMemcpyAsync(buf + o_sk, skeys.data(), (size_t)nsplit * 16, cudaMemcpyHostToDevice, st));
+        DM_CK(cudaMemcpyAsync(buf + o_sp, sprob.data(), (size_t)nsplit * 8, cudaMemcpyHostToDevice, st));
+    }
     const int grid = (count + kDmThreads - 1) / kDmThreads;
     dm_init_kernel<<<grid, kDmThreads, 0, st>>>(a.rng, count, first, (unsigned long long)seed);
     DM_CK(cudaGetLastError());
@@ -396,7 +572,7 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
             for (int k = 0; k < steps; ++k) DM_CK(step());
         }
     }
-    unsigned long long h_stats[6];
+    unsigned long long h_stats[10];
     int status = 0;
     DM_CK(cudaMemcpyAsync(h_stats, a.stats, sizeof(h_stats), cudaMemcpyDeviceToHost, st));
     DM_CK(cudaMemcpyAsync(&status, v.status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -429,7 +605,7 @@ extern "C" int smccat_branch_sweep(smccat_ctx* c, int32_t first, int32_t count, 
         }
     }
     if (stats)
-        for (int k = 0; k < 6; ++k) stats[k] = (int64_t)h_stats[k];
+        for (int k = 0; k < 10; ++k) stats[k] = (int64_t)h_stats[k];
     return finish(SMCCAT_OK, "");
 #undef DM_CK
 }

@@ -97,5 +97,8 @@ bool rebuild_tree(int T, const int32_t* parent, Mirror* m);
 // Device buffer of at least `bytes` owned by the context (kept between calls,
 // reallocated only to grow; freed with the context). nullptr if out of memory.
 unsigned char* moves_buffer(smccat_ctx* c, size_t bytes);
+// The adaptive-NNI split table in use: canonical splits (2 words each) sorted
+// by (word 0, word 1), with their posterior probabilities.
+void split_table(const smccat_ctx* c, std::vector<uint64_t>* keys, std::vector<double>* prob);
 
 }  // namespace smccat

@@ -420,6 +420,21 @@ void mcmc_release(const smccat_ctx* c) {
     tunings().erase(c);
 }
 
+void split_table(const smccat_ctx* c, std::vector<uint64_t>* keys, std::vector<double>* prob) {
+    const auto& mp = tuning_of(c).split_post;
+    std::vector<std::pair<Split, double>> v(mp.begin(), mp.end());
+    std::sort(v.begin(), v.end(), [](const auto& x, const auto& y) {
+        return x.first.w[0] != y.first.w[0] ? x.first.w[0] < y.first.w[0] : x.first.w[1] < y.first.w[1];
+    });
+    keys->resize(2 * v.size());
+    prob->resize(v.size());
+    for (size_t i = 0; i < v.size(); ++i) {
+        (*keys)[2 * i] = v[i].first.w[0];
+        (*keys)[2 * i + 1] = v[i].first.w[1];
+        (*prob)[i] = v[i].second;
+    }
+}
+
 }  // namespace smccat
 
 using namespace smccat;

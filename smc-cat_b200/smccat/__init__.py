@@ -135,7 +135,7 @@ def lib():
         "smccat_ln_prior": ([vp, _i32, _i32, _dp], ctypes.c_int),
         "smccat_resample_tune": ([vp, _i32, _i32, _dp, ctypes.c_double, _i32, _ip], ctypes.c_int),
         "smccat_get_rate_cholesky": ([vp, _dp], ctypes.c_int),
-        "smccat_branch_sweep": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64, _i32,
+        "smccat_tree_sweep": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64, _i32,
                                  ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "smccat_propose": ([vp, _i32, _i32, ctypes.c_uint64, _ip, _dp], ctypes.c_int),
         "smccat_rejuvenate": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64,
@@ -368,16 +368,19 @@ class Engine:
         m = min(cap, n.value)
         return bits[:m], prob[:m]
 
-    def branch_sweep(self, steps, temperature, seed, use_graph=True, first=0, count=None) -> dict:
-        """Branch-length and NNI MCMC steps entirely on the device (one CUDA graph)."""
+    def tree_sweep(self, steps, temperature, seed, use_graph=True, first=0, count=None) -> dict:
+        """Tree-move MCMC steps (the reference's treeMove mixture) entirely on
+        the device, one CUDA graph; returns proposed / accepted per move kind."""
         count = self.P - first if count is None else count
-        st = np.zeros(6, dtype=np.int64)
-        _check(lib().smccat_branch_sweep(self._h, int(first), int(count), int(steps),
-                                         float(temperature), int(seed), 1 if use_graph else 0,
-                                         st.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
-        return {"branch_proposed": int(st[0]), "branch_accepted": int(st[1]),
-                "subtree_proposed": int(st[2]), "subtree_accepted": int(st[3]),
-                "nni_proposed": int(st[4]), "nni_accepted": int(st[5])}
+        st = np.zeros(10, dtype=np.int64)
+        _check(lib().smccat_tree_sweep(self._h, int(first), int(count), int(steps),
+                                       float(temperature), int(seed), 1 if use_graph else 0,
+                                       st.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        out = {}
+        for k, name in enumerate(("adaptive_nni", "nni", "spr", "branch", "subtree")):
+            out[name + "_proposed"] = int(st[2 * k])
+            out[name + "_accepted"] = int(st[2 * k + 1])
+        return out
 
     def rate_cholesky(self) -> np.ndarray:
         out = np.zeros((190, 190))
