@@ -47,7 +47,8 @@
 namespace smccat {
 namespace {
 
-constexpr int kDmThreads = 64;
+constexpr int kDmThreads = 64;  // one thread per particle (generator set-up)
+constexpr int kDmWarps = 4;     // particles per proposal / MH block (one warp each)
 constexpr int kUndo = 8;  // table edits of one move (SPR: 6, NNI: 4)
 
 // Move kinds, numbered like SMCCAT_MOVE_*.
@@ -66,15 +67,11 @@ struct DmArgs {
     uint8_t* cur_clws;   // [count][N] workspaces of this step's proposal
     uint8_t* cur_pws;
     uint8_t* dirty;      // [count][N] bit 0: P, bit 1: partial, bit 2: on the first path
-    int32_t* stack;      // [count][N] walks
-    int32_t* order;      // [count][N] dirty internal nodes, children first
     int32_t* undo_node;  // [count][N] scaled nodes, walk order
     double* undo_len;    // [count][N] their previous lengths
     int32_t* nundo;      // [count]
     int32_t* kind;       // [count] SMCCAT_MOVE_* of this step's move
     double* extra;       // [count] lnPrior change + log Hastings ratio
-    uint64_t* clade;     // [count][N][2] taxa below each node (adaptive NNI)
-    double* wnode;       // [count][N] adaptive-NNI node weights
     const uint64_t* skeys;  // [nsplit][2] canonical splits, sorted
     const double* sprob;    // [nsplit]
     int nsplit;
@@ -124,212 +121,270 @@ __device__ double anni_weight(const DmArgs& a, uint64_t c0, uint64_t c1) {
     return v + (pr >= 0.0 ? 1.0 - pr : 1.0);
 }
 
-__global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.count) return;
+// Shared-memory bytes one particle's proposal needs (per warp).
+__host__ __device__ inline size_t dm_warp_bytes(int N) {
+    return ((size_t)N * (8 + 16 + 8 + 4 * 6 + 3) + 15) & ~size_t(15);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One warp per particle. The particle's tables are staged in shared memory;
+// lane 0 makes the move (the tree walks are sequential), the lanes share the
+// O(N) passes, the adaptive-NNI split lookups and the plan writes.
+__global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
+    extern __shared__ __align__(16) unsigned char dm_smem[];
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (i >= a.count) return;  // whole warps leave together
     const Dims& d = a.d;
     const int N = d.N, T = d.T, NI = d.NI;
-    int32_t* par = a.parent + (size_t)i * N;
-    int32_t* kids = a.kids + (size_t)i * 2 * N;
-    double* br = a.branch + (size_t)i * N;
-    uint8_t* dirty = a.dirty + (size_t)i * N;
-    int32_t* stk = a.stack + (size_t)i * N;
-    int32_t* ord = a.order + (size_t)i * N;
-    int32_t* un = a.undo_node + (size_t)i * N;
-    double* ul = a.undo_len + (size_t)i * N;
-    int32_t* lg = a.ulog + (size_t)i * 2 * kUndo;
+    unsigned char* base = dm_smem + (size_t)(threadIdx.x >> 5) * dm_warp_bytes(N);
+    double* br = reinterpret_cast<double*>(base);     // N
+    uint64_t* cl = reinterpret_cast<uint64_t*>(br + N);  // 2N
+    double* wn = reinterpret_cast<double*>(cl + 2 * N);  // N
+    int32_t* par = reinterpret_cast<int32_t*>(wn + N);   // N
+    int32_t* kids = par + N;                             // 2N
+    int32_t* stk = kids + 2 * N;                         // N
+    int32_t* ord = stk + N;                              // N
+    int32_t* un = ord + N;                               // N
+    uint8_t* dirty = reinterpret_cast<uint8_t*>(un + N); // N
+    uint8_t* cc = dirty + N;                             // N
+    uint8_t* cp = cc + N;                                // N
+    int32_t* gpar = a.parent + (size_t)i * N;
+    int32_t* gkids = a.kids + (size_t)i * 2 * N;
+    double* gbr = a.branch + (size_t)i * N;
     const PartHdr h0 = a.hdr0[i];
     const int root = h0.root;
-    curandStatePhilox4_32_10_t rs = a.rng[i];
-    auto unif = [&]() { return 1.0 - curand_uniform_double(&rs); };  // [0, 1)
-    auto uniform_node = [&]() { return min(N - 1, (int)(unif() * N)); };
-    // A uniform node other than the root (internal only if `internal`); after
-    // 64 misses the first admissible id (probability below 1e-12 for T >= 3).
-    auto pick = [&](bool internal) {
-        int x = root;
-        for (int t = 0; t < 64 && (x == root || (internal && x < T)); ++t) x = uniform_node();
-        if (x == root || (internal && x < T))
-            for (int n = internal ? T : 0; n < N; ++n)
-                if (n != root) { x = n; break; }
-        return x;
-    };
-    auto in_subtree = [&](int y, int r) {  // Tree.hpp:29-34
-        for (int g = 0; y >= 0 && g <= N; y = par[y], ++g)
-            if (y == r) return true;
-        return false;
-    };
-    int nlog = 0;
-    auto set_par = [&](int n, int v) {
-        lg[2 * nlog] = n; lg[2 * nlog + 1] = par[n]; ++nlog;
-        par[n] = v;
-    };
-    auto set_kid = [&](int k, int v) {
-        lg[2 * nlog] = N + k; lg[2 * nlog + 1] = kids[k]; ++nlog;
-        kids[k] = v;
-    };
-    int nord = 0;
-    // Dirty partials on two root paths, recorded children first: the path of
-    // `b` up to where it meets the path of `pa`, then the path of `pa`.
-    auto mark_paths = [&](int pa, int b) {
-        for (int y = pa, g = 0; y >= 0 && g < N; y = par[y], ++g) dirty[y] |= 2 | 4;
-        for (int y = b, g = 0; y >= 0 && g < N && !(dirty[y] & 4); y = par[y], ++g) {
-            dirty[y] |= 2;
-            if (nord < N) ord[nord++] = y;
-        }
-        for (int y = pa, g = 0; y >= 0 && g < N; y = par[y], ++g)
-            if (nord < N) ord[nord++] = y;
-    };
 
-    double L0 = 0.0;
-    for (int n = 0; n < N; ++n) {
+    double l0 = 0.0;
+    for (int n = lane; n < N; n += 32) {
+        par[n] = gpar[n];
+        kids[2 * n] = gkids[2 * n];
+        kids[2 * n + 1] = gkids[2 * n + 1];
+        br[n] = gbr[n];
         dirty[n] = 0;
-        L0 += br[n];
+        l0 += br[n];
     }
-    const double u = unif();  // Particle.cpp:680-701
-    const int kind = u < 0.1 ? kNni : u < 0.4 ? kAnni : u < 0.5 ? kSpr : u < 0.9 ? kBranch : kSubtree;
-    double hastings = 0.0, sc = 1.0;
-    int nch = 0;
-    if (kind == kNni || kind == kAnni) {
-        // NNIMove / adaptiveNNIMove (Tree.cpp:625-766): one child n1 of x
-        // trades places with x's sibling n2; branch lengths stay with their
-        // nodes, so no transition matrix changes.
-        int x;
-        double sel = 0.0, tot = 0.0;
-        double* wn = a.wnode + (size_t)i * N;
-        uint64_t* cl = a.clade + (size_t)i * 2 * N;
-        if (kind == kNni) {
-            x = pick(true);
-        } else {
-            if (a.use_splits) {  // clades bottom-up over a pre-order walk
-                int top = 0, cnt = 0;
-                stk[top++] = root;
-                while (top > 0 && cnt < N) {
-                    const int n = stk[--top];
-                    ord[cnt++] = n;
-                    if (n >= T && top + 2 <= N) { stk[top++] = kids[2 * n]; stk[top++] = kids[2 * n + 1]; }
-                }
-                for (int q = cnt - 1; q >= 0; --q) {
-                    const int n = ord[q];
-                    if (n < T) {
-                        cl[2 * n] = n < 64 ? 1ull << n : 0ull;
-                        cl[2 * n + 1] = n >= 64 ? 1ull << (n - 64) : 0ull;
-                    } else {
-                        const int k1 = kids[2 * n], k2 = kids[2 * n + 1];
-                        cl[2 * n] = cl[2 * k1] | cl[2 * k2];
-                        cl[2 * n + 1] = cl[2 * k1 + 1] | cl[2 * k2 + 1];
-                    }
-                }
-            }
-            for (int n = T; n < N; ++n) {
-                if (n == root) continue;
-                wn[n] = a.use_splits ? anni_weight(a, cl[2 * n], cl[2 * n + 1]) : a.anni_eps + 1.0;
-                tot += wn[n];
-            }
-            const double r = unif();
-            double cum = 0.0;
-            x = -1;
-            for (int n = T; n < N; ++n) {
-                if (n == root) continue;
-                cum += wn[n] / tot;
-                x = n;
-                if (r <= cum) break;
-            }
-            sel = wn[x] / tot;
-        }
-        const int pa = par[x];
-        const int s1 = min(1, (int)(unif() * 2));
-        const int n1 = kids[2 * x + s1];
-        const int s2 = kids[2 * pa] == x ? 1 : 0;
-        const int n2 = kids[2 * pa + s2];
-        set_par(n1, pa);
-        set_par(n2, x);
-        set_kid(2 * pa + s2, n1);
-        set_kid(2 * x + s1, n2);
-        if (kind == kAnni) {
-            // Only x's clade changes: it loses n1's taxa and gains n2's.
-            double w2 = a.anni_eps + 1.0;
-            if (a.use_splits)
-                w2 = anni_weight(a, (cl[2 * x] & ~cl[2 * n1]) | cl[2 * n2],
-                                 (cl[2 * x + 1] & ~cl[2 * n1 + 1]) | cl[2 * n2 + 1]);
-            double tot2 = 0.0;
-            for (int n = T; n < N; ++n)
-                if (n != root) tot2 += n == x ? w2 : wn[n];
-            hastings = log(w2 / tot2) - log(sel);
-        }
-        mark_paths(pa, x);
-    } else if (kind == kSpr) {
-        // SPRMove (Tree.cpp:768-812): prune the subtree of x's child sch (x
-        // comes with it, x's other child sib takes x's place) and regraft x
-        // on the branch above a node an outside it.
-        const int x = pick(true);
-        const int s1 = min(1, (int)(unif() * 2));
-        const int sib = kids[2 * x + 1 - s1];
-        int an = -1;
-        for (int t = 0; t < 256 && an < 0; ++t) {
-            const int c = uniform_node();
-            if (c != root && !in_subtree(c, x)) an = c;
-        }
-        if (an < 0)  // x's parent or sibling always qualifies
-            for (int n = 0; n < N && an < 0; ++n)
-                if (n != root && !in_subtree(n, x)) an = n;
-        const int gp = par[x];
-        set_kid(2 * gp + (kids[2 * gp] == x ? 0 : 1), sib);
-        set_par(sib, gp);
-        const int ap = par[an];
-        set_kid(2 * ap + (kids[2 * ap] == an ? 0 : 1), x);
-        set_par(x, ap);
-        set_kid(2 * x + 1 - s1, an);
-        set_par(an, x);
-        mark_paths(gp, x);
-    } else {
-        // scaleBranchMove / scaleSubtreeMove (Tree.cpp:553-612): x's branch,
-        // or every branch of x's subtree (walk order: pre-order with the
-        // second child first; reversed it is a post-order).
-        const bool subtree = kind == kSubtree;
-        const int x = pick(false);
-        sc = exp((subtree ? a.subtree_delta : a.scale_delta) * (unif() - 0.5));
-        int top = 0;
-        stk[top++] = x;
-        while (top > 0) {  // every node is pushed once: top <= N, nch <= N
-            const int n = stk[--top];
-            un[nch] = n;
-            ul[nch] = br[n];
-            ++nch;
-            br[n] *= sc;
-            dirty[n] |= 1;
-            if (subtree && n >= T) {
-                stk[top++] = kids[2 * n];
-                stk[top++] = kids[2 * n + 1];
-            }
-        }
-        if (subtree)
-            for (int q = nch - 1; q >= 0; --q)
-                if (un[q] >= T) {
-                    dirty[un[q]] |= 2;
-                    if (nord < N) ord[nord++] = un[q];
-                }
-        for (int y = par[x], g = 0; y >= 0 && g < N; y = par[y], ++g) {
-            dirty[y] |= 2;
-            if (nord < N) ord[nord++] = y;
-        }
-        hastings = nch * log(sc);
-    }
-    a.nlog[i] = nlog;
-    a.nundo[i] = nch;
-    a.kind[i] = kind;
+    const double L0 = warp_sum(l0);
+    __syncwarp();
 
+    curandStatePhilox4_32_10_t rs;
+    int kind = 0;
+    if (lane == 0) {
+        rs = a.rng[i];
+        const double u = 1.0 - curand_uniform_double(&rs);  // Particle.cpp:680-701
+        kind = u < 0.1 ? kNni : u < 0.4 ? kAnni : u < 0.5 ? kSpr : u < 0.9 ? kBranch : kSubtree;
+        if (kind == kAnni && a.use_splits) {  // clades bottom-up over a pre-order walk
+            int top = 0, cnt = 0;
+            stk[top++] = root;
+            while (top > 0 && cnt < N) {
+                const int n = stk[--top];
+                ord[cnt++] = n;
+                if (n >= T && top + 2 <= N) { stk[top++] = kids[2 * n]; stk[top++] = kids[2 * n + 1]; }
+            }
+            for (int q = cnt - 1; q >= 0; --q) {
+                const int n = ord[q];
+                if (n < T) {
+                    cl[2 * n] = n < 64 ? 1ull << n : 0ull;
+                    cl[2 * n + 1] = n >= 64 ? 1ull << (n - 64) : 0ull;
+                } else {
+                    const int k1 = kids[2 * n], k2 = kids[2 * n + 1];
+                    cl[2 * n] = cl[2 * k1] | cl[2 * k2];
+                    cl[2 * n + 1] = cl[2 * k1 + 1] | cl[2 * k2 + 1];
+                }
+            }
+        }
+    }
+    kind = __shfl_sync(0xffffffffu, kind, 0);
+    __syncwarp();
+    if (kind == kAnni) {  // node weights, the lookups spread over the lanes
+        for (int n = T + lane; n < N; n += 32)
+            if (n != root) wn[n] = a.use_splits ? anni_weight(a, cl[2 * n], cl[2 * n + 1]) : a.anni_eps + 1.0;
+        __syncwarp();
+    }
+
+    int nord = 0, nch = 0;
+    double hastings = 0.0;
+    if (lane == 0) {
+        int32_t* lg = a.ulog + (size_t)i * 2 * kUndo;
+        double* gul = a.undo_len + (size_t)i * N;
+        auto unif = [&]() { return 1.0 - curand_uniform_double(&rs); };  // [0, 1)
+        auto uniform_node = [&]() { return min(N - 1, (int)(unif() * N)); };
+        // A uniform node other than the root (internal only if `internal`);
+        // after 64 misses the first admissible id (probability below 1e-12).
+        auto pick = [&](bool internal) {
+            int x = root;
+            for (int t = 0; t < 64 && (x == root || (internal && x < T)); ++t) x = uniform_node();
+            if (x == root || (internal && x < T))
+                for (int n = internal ? T : 0; n < N; ++n)
+                    if (n != root) { x = n; break; }
+            return x;
+        };
+        auto in_subtree = [&](int y, int r) {  // Tree.hpp:29-34
+            for (int g = 0; y >= 0 && g <= N; y = par[y], ++g)
+                if (y == r) return true;
+            return false;
+        };
+        int nlog = 0;
+        auto set_par = [&](int n, int v) {
+            lg[2 * nlog] = n; lg[2 * nlog + 1] = par[n]; ++nlog;
+            par[n] = v;
+        };
+        auto set_kid = [&](int k, int v) {
+            lg[2 * nlog] = N + k; lg[2 * nlog + 1] = kids[k]; ++nlog;
+            kids[k] = v;
+        };
+        // Dirty partials on two root paths, recorded children first: the path
+        // of `b` up to where it meets the path of `pa`, then the path of `pa`.
+        auto mark_paths = [&](int pa, int b) {
+            for (int y = pa, g = 0; y >= 0 && g < N; y = par[y], ++g) dirty[y] |= 2 | 4;
+            for (int y = b, g = 0; y >= 0 && g < N && !(dirty[y] & 4); y = par[y], ++g) {
+                dirty[y] |= 2;
+                if (nord < N) ord[nord++] = y;
+            }
+            for (int y = pa, g = 0; y >= 0 && g < N; y = par[y], ++g)
+                if (nord < N) ord[nord++] = y;
+        };
+
+        if (kind == kNni || kind == kAnni) {
+            // NNIMove / adaptiveNNIMove (Tree.cpp:625-766): one child n1 of x
+            // trades places with x's sibling n2; branch lengths stay with
+            // their nodes, so no transition matrix changes.
+            int x;
+            double sel = 0.0, tot = 0.0;
+            if (kind == kNni) {
+                x = pick(true);
+            } else {
+                for (int n = T; n < N; ++n)
+                    if (n != root) tot += wn[n];
+                const double r = unif();
+                double cum = 0.0;
+                x = -1;
+                for (int n = T; n < N; ++n) {
+                    if (n == root) continue;
+                    cum += wn[n] / tot;
+                    x = n;
+                    if (r <= cum) break;
+                }
+                sel = wn[x] / tot;
+            }
+            const int pa = par[x];
+            const int s1 = min(1, (int)(unif() * 2));
+            const int n1 = kids[2 * x + s1];
+            const int s2 = kids[2 * pa] == x ? 1 : 0;
+            const int n2 = kids[2 * pa + s2];
+            set_par(n1, pa);
+            set_par(n2, x);
+            set_kid(2 * pa + s2, n1);
+            set_kid(2 * x + s1, n2);
+            if (kind == kAnni) {
+                // Only x's clade changes: it loses n1's taxa and gains n2's.
+                double w2 = a.anni_eps + 1.0;
+                if (a.use_splits)
+                    w2 = anni_weight(a, (cl[2 * x] & ~cl[2 * n1]) | cl[2 * n2],
+                                     (cl[2 * x + 1] & ~cl[2 * n1 + 1]) | cl[2 * n2 + 1]);
+                double tot2 = 0.0;
+                for (int n = T; n < N; ++n)
+                    if (n != root) tot2 += n == x ? w2 : wn[n];
+                hastings = log(w2 / tot2) - log(sel);
+            }
+            mark_paths(pa, x);
+        } else if (kind == kSpr) {
+            // SPRMove (Tree.cpp:768-812): prune the subtree of x's child (x
+            // comes with it, x's other child sib takes x's place) and regraft
+            // x on the branch above a node an outside it.
+            const int x = pick(true);
+            const int s1 = min(1, (int)(unif() * 2));
+            const int sib = kids[2 * x + 1 - s1];
+            int an = -1;
+            for (int t = 0; t < 256 && an < 0; ++t) {
+                const int c = uniform_node();
+                if (c != root && !in_subtree(c, x)) an = c;
+            }
+            if (an < 0)  // x's parent or sibling always qualifies
+                for (int n = 0; n < N && an < 0; ++n)
+                    if (n != root && !in_subtree(n, x)) an = n;
+            const int gp = par[x];
+            set_kid(2 * gp + (kids[2 * gp] == x ? 0 : 1), sib);
+            set_par(sib, gp);
+            const int ap = par[an];
+            set_kid(2 * ap + (kids[2 * ap] == an ? 0 : 1), x);
+            set_par(x, ap);
+            set_kid(2 * x + 1 - s1, an);
+            set_par(an, x);
+            mark_paths(gp, x);
+        } else {
+            // scaleBranchMove / scaleSubtreeMove (Tree.cpp:553-612): x's
+            // branch, or every branch of x's subtree (walk order: pre-order
+            // with the second child first; reversed it is a post-order).
+            const bool subtree = kind == kSubtree;
+            const int x = pick(false);
+            const double sc = exp((subtree ? a.subtree_delta : a.scale_delta) * (unif() - 0.5));
+            int top = 0;
+            stk[top++] = x;
+            while (top > 0) {  // every node is pushed once: top <= N, nch <= N
+                const int n = stk[--top];
+                un[nch] = n;
+                gul[nch] = br[n];
+                ++nch;
+                br[n] *= sc;
+                dirty[n] |= 1;
+                if (subtree && n >= T) {
+                    stk[top++] = kids[2 * n];
+                    stk[top++] = kids[2 * n + 1];
+                }
+            }
+            if (subtree)
+                for (int q = nch - 1; q >= 0; --q)
+                    if (un[q] >= T) {
+                        dirty[un[q]] |= 2;
+                        if (nord < N) ord[nord++] = un[q];
+                    }
+            for (int y = par[x], g = 0; y >= 0 && g < N; y = par[y], ++g) {
+                dirty[y] |= 2;
+                if (nord < N) ord[nord++] = y;
+            }
+            hastings = nch * log(sc);
+        }
+        a.nlog[i] = nlog;
+        a.nundo[i] = nch;
+        a.kind[i] = kind;
+        a.rng[i] = rs;
+    }
+    nord = __shfl_sync(0xffffffffu, nord, 0);
+    nch = __shfl_sync(0xffffffffu, nch, 0);
+    __syncwarp();
+
+    // Next workspaces, the tree and the dirty flags back to global memory.
     const uint8_t* kc = a.clws + (size_t)i * N;
     const uint8_t* kp = a.pws + (size_t)i * N;
-    uint8_t* cc = a.cur_clws + (size_t)i * N;
-    uint8_t* cp = a.cur_pws + (size_t)i * N;
-    for (int n = 0; n < N; ++n) {
-        cc[n] = (dirty[n] & 2) ? 1 - kc[n] : kc[n];
-        cp[n] = (dirty[n] & 1) ? 1 - kp[n] : kp[n];
+    uint8_t* gcc = a.cur_clws + (size_t)i * N;
+    uint8_t* gcp = a.cur_pws + (size_t)i * N;
+    uint8_t* gdirty = a.dirty + (size_t)i * N;
+    double l1 = 0.0;
+    for (int n = lane; n < N; n += 32) {
+        const uint8_t f = dirty[n];
+        cc[n] = (f & 2) ? 1 - kc[n] : kc[n];
+        cp[n] = (f & 1) ? 1 - kp[n] : kp[n];
+        gcc[n] = cc[n];
+        gcp[n] = cp[n];
+        gdirty[n] = f;
+        gpar[n] = par[n];
+        gkids[2 * n] = kids[2 * n];
+        gkids[2 * n + 1] = kids[2 * n + 1];
+        gbr[n] = br[n];
+        l1 += br[n];
     }
+    const double L1 = warp_sum(l1);
+    __syncwarp();
     // Plan: the recorded dirty internal nodes, each after its dirty children.
     NodeJob* nj = a.nodes + (size_t)i * NI;
-    int nn = 0;
-    for (int q = 0; q < nord && nn < NI; ++q) {
+    const int nn = min(nord, NI);
+    for (int q = lane; q < nn; q += 32) {
         const int n = ord[q];
         const int c1 = kids[2 * n], c2 = kids[2 * n + 1];
         int ws = cc[n];
@@ -337,65 +392,80 @@ __global__ void __launch_bounds__(kDmThreads) dm_propose_kernel(DmArgs a) {
         if (c2 >= T) ws |= cc[c2] << 2;
         ws |= cp[c1] << 3;
         ws |= cp[c2] << 4;
-        nj[nn++] = NodeJob{n, c1, c2, ws};
+        nj[q] = NodeJob{n, c1, c2, ws};
     }
     PJob* pj = a.pjobs + (size_t)i * N;
-    for (int q = 0; q < nch; ++q) pj[q] = PJob{a.first + i, un[q], cp[un[q]], 0, br[un[q]]};
+    int32_t* gun = a.undo_node + (size_t)i * N;
+    for (int q = lane; q < nch; q += 32) {
+        pj[q] = PJob{a.first + i, un[q], cp[un[q]], 0, br[un[q]]};
+        gun[q] = un[q];
+    }
     PmJob* mj = a.mjobs + (size_t)i * d.Kmax * a.nchunk;
-    for (int k = 0; k < d.Kmax; ++k)
-        for (int c = 0; c < a.nchunk; ++c) {
-            const int nj_k = k < h0.num_classes ? max(0, min(kPmChunk, nch - kPmChunk * c)) : 0;
-            mj[k * a.nchunk + c] = PmJob{i, k, i * N + kPmChunk * c, nj_k};
-        }
-    PartHdr h = h0;
-    h.node_off = i * NI;
-    h.node_cnt = nn;
-    h.root_ws = cc[root];
-    h.active = 1;
-    a.hdr[i] = h;
-    double L1 = 0.0;
-    for (int n = 0; n < N; ++n) L1 += br[n];
-    // Tree-length prior Gamma(2T-2, scale 1/10) (Particle.cpp:484-517) and the
-    // Hastings ratio.
-    a.extra[i] = (N - 2) * (log(L1) - log(L0)) - (L1 - L0) / 0.1 + hastings;
-    a.rng[i] = rs;
+    for (int e = lane; e < d.Kmax * a.nchunk; e += 32) {
+        const int k = e / a.nchunk, c = e - k * a.nchunk;
+        const int nj_k = k < h0.num_classes ? max(0, min(kPmChunk, nch - kPmChunk * c)) : 0;
+        mj[e] = PmJob{i, k, i * N + kPmChunk * c, nj_k};
+    }
+    if (lane == 0) {
+        PartHdr h = h0;
+        h.node_off = i * NI;
+        h.node_cnt = nn;
+        h.root_ws = cc[root];
+        h.active = 1;
+        a.hdr[i] = h;
+        // Tree-length prior Gamma(2T-2, scale 1/10) (Particle.cpp:484-517)
+        // and the Hastings ratio.
+        a.extra[i] = (N - 2) * (log(L1) - log(L0)) - (L1 - L0) / 0.1 + hastings;
+    }
 }
 
-__global__ void __launch_bounds__(kDmThreads) dm_mh_kernel(DmArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.count) return;
+// One warp per particle: lane 0 draws the decision, the lanes commit the
+// workspaces or restore the branch lengths; lane 0 replays the table log.
+__global__ void __launch_bounds__(kDmWarps * 32) dm_mh_kernel(DmArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (i >= a.count) return;  // whole warps leave together
     const int N = a.d.N, p = a.first + i;
-    curandStatePhilox4_32_10_t rs = a.rng[i];
-    const double ratio = a.temp * (a.lnl[p] - a.lnl_old[p]) + a.extra[i];
-    const bool ok = log(curand_uniform_double(&rs)) <= ratio;  // NaN ratios reject
-    const uint8_t* dirty = a.dirty + (size_t)i * N;
     const int kind = a.kind[i];
-    atomicAdd(&a.stats[2 * kind], 1ull);
+    int ok = 0;
+    if (lane == 0) {
+        curandStatePhilox4_32_10_t rs = a.rng[i];
+        const double ratio = a.temp * (a.lnl[p] - a.lnl_old[p]) + a.extra[i];
+        ok = log(curand_uniform_double(&rs)) <= ratio;  // NaN ratios reject
+        a.rng[i] = rs;
+        atomicAdd(&a.stats[2 * kind], 1ull);
+        if (ok) {
+            a.lnl_old[p] = a.lnl[p];
+            atomicAdd(&a.stats[2 * kind + 1], 1ull);
+        } else {
+            a.lnl[p] = a.lnl_old[p];
+            int32_t* par = a.parent + (size_t)i * N;
+            int32_t* kids = a.kids + (size_t)i * 2 * N;
+            const int32_t* lg = a.ulog + (size_t)i * 2 * kUndo;
+            for (int q = a.nlog[i] - 1; q >= 0; --q) {
+                const int x = lg[2 * q];
+                if (x < N) par[x] = lg[2 * q + 1];
+                else kids[x - N] = lg[2 * q + 1];
+            }
+        }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
     if (ok) {
-        a.lnl_old[p] = a.lnl[p];
+        const uint8_t* dirty = a.dirty + (size_t)i * N;
         uint8_t* kc = a.clws + (size_t)i * N;
         uint8_t* kp = a.pws + (size_t)i * N;
-        for (int n = 0; n < N; ++n) {
-            if (dirty[n] & 2) kc[n] = a.cur_clws[(size_t)i * N + n];
-            if (dirty[n] & 1) kp[n] = a.cur_pws[(size_t)i * N + n];
+        for (int n = lane; n < N; n += 32) {
+            const uint8_t f = dirty[n];
+            if (f & 2) kc[n] = a.cur_clws[(size_t)i * N + n];
+            if (f & 1) kp[n] = a.cur_pws[(size_t)i * N + n];
         }
-        atomicAdd(&a.stats[2 * kind + 1], 1ull);
     } else {
-        a.lnl[p] = a.lnl_old[p];
+        // The scaled nodes are distinct: their lengths restore in any order.
         double* br = a.branch + (size_t)i * N;
         const int32_t* un = a.undo_node + (size_t)i * N;
         const double* ul = a.undo_len + (size_t)i * N;
-        for (int q = a.nundo[i] - 1; q >= 0; --q) br[un[q]] = ul[q];
-        int32_t* par = a.parent + (size_t)i * N;
-        int32_t* kids = a.kids + (size_t)i * 2 * N;
-        const int32_t* lg = a.ulog + (size_t)i * 2 * kUndo;
-        for (int q = a.nlog[i] - 1; q >= 0; --q) {
-            const int x = lg[2 * q];
-            if (x < N) par[x] = lg[2 * q + 1];
-            else kids[x - N] = lg[2 * q + 1];
-        }
+        for (int q = lane; q < a.nundo[i]; q += 32) br[un[q]] = ul[q];
     }
-    a.rng[i] = rs;
 }
 
 int dm_fail(int code, const std::string& msg) {
@@ -470,10 +540,9 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
     auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 255) & ~size_t(255); return o; };
     const size_t cN = (size_t)count * N;
     const size_t o_par = take(cN * 4), o_kids = take(2 * cN * 4), o_log = take((size_t)count * 2 * kUndo * 4),
-                 o_nlog = take((size_t)count * 4), o_ord = take(cN * 4), o_clade = take(2 * cN * 8),
-                 o_wn = take(cN * 8), o_sk = take((size_t)std::max(nsplit, 1) * 16),
+                 o_nlog = take((size_t)count * 4), o_sk = take((size_t)std::max(nsplit, 1) * 16),
                  o_sp = take((size_t)std::max(nsplit, 1) * 8), o_br = take(cN * 8), o_clws = take(cN),
-                 o_pws = take(cN), o_cc = take(cN), o_cp = take(cN), o_dirty = take(cN), o_stack = take(cN * 4),
+                 o_pws = take(cN), o_cc = take(cN), o_cp = take(cN), o_dirty = take(cN),
                  o_un = take(cN * 4), o_ul = take(cN * 8), o_nundo = take((size_t)count * 4),
                  o_kind = take((size_t)count * 4), o_extra = take((size_t)count * 8),
                  o_hdr0 = take((size_t)count * sizeof(PartHdr)), o_hdr = take((size_t)count * sizeof(PartHdr)),
@@ -486,9 +555,6 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
     a.kids = reinterpret_cast<int32_t*>(buf + o_kids);
     a.ulog = reinterpret_cast<int32_t*>(buf + o_log);
     a.nlog = reinterpret_cast<int32_t*>(buf + o_nlog);
-    a.order = reinterpret_cast<int32_t*>(buf + o_ord);
-    a.clade = reinterpret_cast<uint64_t*>(buf + o_clade);
-    a.wnode = reinterpret_cast<double*>(buf + o_wn);
     a.skeys = reinterpret_cast<const uint64_t*>(buf + o_sk);
     a.sprob = reinterpret_cast<const double*>(buf + o_sp);
     a.branch = reinterpret_cast<double*>(buf + o_br);
@@ -497,7 +563,6 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
     a.cur_clws = buf + o_cc;
     a.cur_pws = buf + o_cp;
     a.dirty = buf + o_dirty;
-    a.stack = reinterpret_cast<int32_t*>(buf + o_stack);
     a.undo_node = reinterpret_cast<int32_t*>(buf + o_un);
     a.undo_len = reinterpret_cast<double*>(buf + o_ul);
     a.nundo = reinterpret_cast<int32_t*>(buf + o_nundo);
@@ -538,6 +603,18 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
         DM_CK(cudaMemcpyAsync(buf + o_sp, sprob.data(), (size_t)nsplit * 8, cudaMemcpyHostToDevice, st));
     }
     const int grid = (count + kDmThreads - 1) / kDmThreads;
+    // Proposal blocks: kDmWarps particles each, fewer when their shared
+    // memory would exceed the per-block limit.
+    int dev = 0, smem_max = 0;
+    DM_CK(cudaGetDevice(&dev));
+    DM_CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t wbytes = dm_warp_bytes(N);
+    const int pwarps = (int)std::min<size_t>(kDmWarps, (size_t)smem_max / wbytes);
+    if (pwarps < 1) return finish(SMCCAT_EINVAL, "too many taxa for the device tree sweep");
+    const size_t psmem = (size_t)pwarps * wbytes;
+    if (psmem > 48 * 1024)
+        DM_CK(cudaFuncSetAttribute(dm_propose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem));
+    const int pgrid = (count + pwarps - 1) / pwarps;
     dm_init_kernel<<<grid, kDmThreads, 0, st>>>(a.rng, count, first, (unsigned long long)seed);
     DM_CK(cudaGetLastError());
     DM_CK(cudaStreamSynchronize(st));  // the host images may go out of scope only after their copies
@@ -547,13 +624,13 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
     pa.nodes = a.nodes;
     const int nmjobs = count * d.Kmax * nchunk;
     auto step = [&]() -> cudaError_t {
-        dm_propose_kernel<<<grid, kDmThreads, 0, st>>>(a);
+        dm_propose_kernel<<<pgrid, 32 * pwarps, psmem, st>>>(a);
         cudaError_t x = cudaGetLastError();
         if (x == cudaSuccess) x = launch_pmat(a.mjobs, nmjobs, a.pjobs, a.hdr, first, v.sws, v.spec, v.Pm, v.fp32, d, st);
         if (x == cudaSuccess) x = launch_prune(pa, v.ntiles, v.variant, st);
         if (x == cudaSuccess) x = launch_reduce(v.tile_off, pa.partial, a.hdr, first, count, v.lnl, v.status, st);
         if (x == cudaSuccess) {
-            dm_mh_kernel<<<grid, kDmThreads, 0, st>>>(a);
+            dm_mh_kernel<<<(count + kDmWarps - 1) / kDmWarps, 32 * kDmWarps, 0, st>>>(a);
             x = cudaGetLastError();
         }
         return x;
