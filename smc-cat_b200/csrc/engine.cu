@@ -459,7 +459,7 @@ int smccat_set_particles(smccat_ctx* c, int32_t first, int32_t count, const int3
     // the first bad particle in index order is reported).
     std::vector<Mirror> trees(count);
     std::vector<uint8_t> bad(count, 0);
-#pragma omp parallel for schedule(static) if (count >= kParallelParticles)
+#pragma omp parallel for schedule(static) num_threads(host_team()) if (count >= kParallelParticles)
     for (int i = 0; i < count; ++i) {
         uint8_t why = 0;
         const int K = num_classes[i];
@@ -494,7 +494,7 @@ int smccat_set_particles(smccat_ctx* c, int32_t first, int32_t count, const int3
     }
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaEventSynchronize(c->plan_done));  // h_perm may still be in flight
-#pragma omp parallel for schedule(static) if (count >= kParallelParticles)
+#pragma omp parallel for schedule(static) num_threads(host_team()) if (count >= kParallelParticles)
     for (int i = 0; i < count; ++i) {
         const int p = first + i;
         Slot& s = c->slots[p];

@@ -6,7 +6,10 @@
 #include <cstdint>
 #include <string>
 #include <utility>
+#include <algorithm>
 #include <vector>
+
+#include <omp.h>
 
 #include "kernels.h"
 #include "smccat.h"
@@ -17,6 +20,13 @@ namespace smccat {
 // proposals and MH tests) run on OpenMP threads; each iteration touches only
 // its own particle's slot.
 constexpr int kParallelParticles = 32;
+// Host threads for per-particle loops: a quarter of the cores stay free for
+// the caller's and the CUDA driver's threads (a full team that loses one core
+// to them stalls every parallel region for a scheduler time slice).
+inline int host_team() {
+    const int t = omp_get_max_threads();
+    return std::max(1, t - std::max(1, t / 4));
+}
 constexpr int kPackThreads = 4;  // threads packing a refresh plan
 
 // Host mirror of one particle's state and of its device workspace indices.

@@ -716,7 +716,7 @@ int smccat_rejuvenate(smccat_ctx* c, int32_t first, int32_t count, int32_t itera
     std::vector<double> lnl(count);
     rc = smccat_get_lnl(c, first, count, lnl.data());
     if (rc) return rc;
-#pragma omp parallel for schedule(static) if (count >= kParallelParticles)
+#pragma omp parallel for schedule(static) num_threads(host_team()) if (count >= kParallelParticles)
     for (int i = 0; i < count; ++i) {
         ps[i].lik = lnl[i] * temperature;
         ps[i].prior = ln_prior(c, first + i, tn);
@@ -728,7 +728,7 @@ int smccat_rejuvenate(smccat_ctx* c, int32_t first, int32_t count, int32_t itera
     for (;;) {
         // Proposals on the host mirrors; each particle has its own generator
         // and touches only its own slot, so they run in parallel.
-#pragma omp parallel for schedule(dynamic, 8) if (count >= kParallelParticles)
+#pragma omp parallel for schedule(dynamic, 8) num_threads(host_team()) if (count >= kParallelParticles)
         for (int i = 0; i < count; ++i) {
             PS& q = ps[i];
             active[i] = 0;
@@ -763,7 +763,7 @@ int smccat_rejuvenate(smccat_ctx* c, int32_t first, int32_t count, int32_t itera
         rc = smccat_get_lnl(c, first, count, lnl.data());
         if (rc) return rc;
         st.lockstep_steps++;
-#pragma omp parallel for schedule(static) if (count >= kParallelParticles)
+#pragma omp parallel for schedule(static) num_threads(host_team()) if (count >= kParallelParticles)
         for (int i = 0; i < count; ++i)
             if (active[i]) nprior[i] = ln_prior(c, first + i, tn);
         for (int i = 0; i < count; ++i) {
