@@ -39,9 +39,10 @@ cudaError_t launch_pmat(const PmJob* mjobs, int n, const PJob* jobs, const PartH
                         const uint8_t* sws, const double* spec, void* Pm, bool fp32, const Dims& d,
                         cudaStream_t st);
 // Pruning kernel variants available for R rate categories: SIMT kernels at
-// several register caps, then (FP64 only) the FP64 tensor-path kernels.
+// several register caps, then the FP64 tensor-path kernels (FP64) or the
+// tcgen05 3xTF32 kernel (FP32).
 int prune_variants(int R, bool fp32);
-// Slots per pruning tile that a variant expects (32 or 64).
+// Slots per pruning tile that a variant expects (32, 64 or 128).
 int prune_variant_tile_sites(int R, bool fp32, int variant);
 // The variant used until smccat_autotune or smccat_set_kernel_variant picks
 // another: the fastest measured on B200 for the bench workloads.
@@ -49,6 +50,9 @@ int prune_default_variant(int R, bool fp32);
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
 int prune_dmma_variants(int R);
 cudaError_t launch_prune_dmma(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
+// FP32 tensor-core (tcgen05, 3xTF32) kernels: 128-slot tiles.
+int prune_tc_variants(int R);
+cudaError_t launch_prune_tc(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
 cudaError_t launch_reduce(const int32_t* tile_off, const double* partial, const PartHdr* hdr, int first,
                           int count, double* lnl, int* status, cudaStream_t st);
 cudaError_t launch_accept(double* lnl, double* lnl_old, const uint8_t* mask, int first, int count,

@@ -657,10 +657,11 @@ cudaError_t launch_prune_fp32(const PruneArgs& a, int ntiles, int variant, cudaS
 
 }  // namespace
 
-// FP64 contexts also have the tensor-path (DMMA) kernels, numbered after the
-// SIMT ones; they use 32-slot tiles.
+// Numbered after the SIMT kernels: FP64 contexts have the FP64 tensor-path
+// (DMMA) kernels, on 32-slot tiles; FP32 contexts the tcgen05 3xTF32 kernel,
+// on 128-slot tiles.
 int prune_variants(int R, bool fp32) {
-    return simt_variants(R, fp32) + (fp32 ? 0 : prune_dmma_variants(R));
+    return simt_variants(R, fp32) + (fp32 ? prune_tc_variants(R) : prune_dmma_variants(R));
 }
 
 // FP64: one site per lane, four rows in flight (variant 3 at R = 4: 6.76 ms
@@ -673,12 +674,16 @@ int prune_default_variant(int R, bool fp32) {
 
 int prune_variant_tile_sites(int R, bool fp32, int variant) {
     if (variant < simt_variants(R, fp32)) return 32 * simt_width(R, variant);
-    return 32;
+    return fp32 ? 128 : 32;
 }
 
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st) {
     if (ntiles <= 0) return cudaSuccess;
-    if (a.fp32) return launch_prune_fp32(a, ntiles, variant, st);
+    if (a.fp32) {
+        const int ns = simt_variants(a.d.R, true);
+        if (variant >= ns) return launch_prune_tc(a, ntiles, variant - ns, st);
+        return launch_prune_fp32(a, ntiles, variant, st);
+    }
     const int ns = simt_variants(a.d.R, false);
     if (variant >= ns) return launch_prune_dmma(a, ntiles, variant - ns, st);
     return launch_prune_typed<double>(a, ntiles, variant, st);
