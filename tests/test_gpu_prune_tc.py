@@ -113,3 +113,17 @@ def test_tc_variant_is_in_the_autotuner():
     for i in range(cfg.particles):
         assert abs(got[i] - oracle_lnl(codes, cfg, st, i)) < FP32_ATOL
     eng.close()
+
+
+def test_tc_kernel_inside_the_device_tree_sweep():
+    cfg = CFGS[0]
+    eng, codes, st = engine(cfg)
+    eng.set_kernel_variant(tc_variant(eng))
+    eng.refresh(full=True)
+    stats = eng.tree_sweep(steps=12, temperature=0.9, seed=8)
+    assert sum(v for k, v in stats.items() if k.endswith("_proposed")) == 12 * cfg.particles
+    fin = eng.get_particles()
+    got = eng.lnl()
+    for i in range(cfg.particles):
+        assert abs(got[i] - oracle_lnl(codes, cfg, fin, i)) < FP32_ATOL
+    eng.close()
