@@ -204,3 +204,19 @@ def test_tree_sweep_refuses_uncommitted_edits():
         eng.tree_sweep(steps=1, temperature=1.0, seed=1)
     assert e.value.code == smccat.ESTATE
     eng.close()
+
+
+def test_tree_sweep_on_three_taxa():
+    # The smallest tree: one internal non-root node, so NNI and SPR have a
+    # single admissible target node and a single regraft point.
+    cfg = workload.WorkloadConfig("dm_t3", T=3, S=40, R=2, particles=4, iterations=1, lg=True,
+                                  invar=False, cat=False, alpha=0.9, seed=2)
+    eng, codes, st = engine(cfg)
+    stats = eng.tree_sweep(steps=20, temperature=0.5, seed=3)
+    assert sum(stats[k + "_proposed"] for k in KINDS) == 20 * cfg.particles
+    fin = eng.get_particles()
+    got = eng.lnl()
+    for i in range(cfg.particles):
+        assert (fin["parent"][i] < 0).sum() == 1
+        assert got[i] == pytest.approx(oracle_lnl(codes, cfg, fin, i), rel=1e-9)
+    eng.close()

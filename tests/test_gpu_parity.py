@@ -369,3 +369,25 @@ def test_reference_configs_full_size(cid):
                            st["logits"], st["assign"], st["pinv"], rates)
     np.testing.assert_allclose(got, ref, rtol=RTOL)
     eng.close()
+
+
+@pytest.mark.parametrize("cfg", SMALL, ids=lambda c: c.name)
+def test_every_fp32_variant_matches_oracle(cfg):
+    """Each FP32 pruning variant (SIMT register caps and the tcgen05 3xTF32
+    kernel) within the FP32 tolerance, R = 1 .. 8 and T = 3 included."""
+    rng = np.random.default_rng(cfg.seed + 7)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    st = workload.make_particles(cfg, cfg.particles, rng)
+    eng = smccat.Engine(codes, cfg.R, cfg.particles, max_classes=st["logits"].shape[1],
+                        lg=cfg.lg, invar=cfg.invar, cat=cfg.cat, precision=smccat.PREC_FP32)
+    nv, _ = eng.kernel_variants()
+    refs = [oracle_lnl(codes, st, i, cfg.R)[0] for i in range(cfg.particles)]
+    for v in range(nv):
+        eng.set_kernel_variant(v)
+        eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                          st["logits"], st["assign"], st["pinv"], st["shape"])
+        eng.refresh(full=True)
+        got = eng.lnl()
+        for i in range(cfg.particles):
+            assert abs(got[i] - refs[i]) <= MIXED_ATOL, (v, i, got[i] - refs[i])
+    eng.close()
