@@ -20,6 +20,7 @@
 //                 log-sum-exp over rates, +I, warp sum.
 //   reduce_kernel per particle, sums the tile partials in a fixed order.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <math.h>
 
 #include "kernels.h"
@@ -272,14 +273,14 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
 // T = storage and arithmetic type of partials and transition matrices
 // (double, or float for the mixed-precision path); log-scalers and the root
 // reduction are FP64 in both.
+// One tile. `phase` holds each P buffer's next barrier parity; the barriers
+// are initialised when `init` is set (a CTA's first tile) and reused after.
 template <class T, int R, int MINB, int W, int RB>
-__global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) {
+__device__ __forceinline__ void prune_tile(const PruneArgs& a, const int tile_id, uint32_t& phase, bool init) {
     const Dims d = a.d;
-    const int tile_id = a.tile_begin + blockIdx.x;
     const Tile tl = a.tiles[tile_id];
     const int p = tl.p;
     const PartHdr* h = a.hdr + (p - a.first);
-    if (!h->active) return;  // uniform across the CTA
     constexpr uint32_t kPBytes = kPBlock * sizeof(T);
 
     extern __shared__ __align__(128) unsigned char smem_raw[];  // [R warps][2 buffers][2 children][kPBlock]
@@ -321,16 +322,18 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     };
 
     if (threadIdx.x == 0) bad = 0;
-    if (lane == 0) {
+    if (init && lane == 0) {
         mbar_init(&bars[r][0], 1);
         mbar_init(&bars[r][1], 1);
         fence_mbar_init();
     }
     __syncthreads();
+    if (!h->active) return;  // uniform across the CTA (after the barriers exist)
 
     const int cnt = h->node_cnt;
     const NodeJob* nodes = a.nodes + h->node_off;
     if (cnt > 0 && lane == 0) {
+        fence_proxy_async();  // a previous tile's root rows were written here
         const NodeJob nj = nodes[0];
         mbar_expect_tx(&bars[r][0], 2 * kPBytes);
         tma_load_1d(buf, pblock(nj.c1, (nj.ws >> 3) & 1), kPBytes, &bars[r][0]);
@@ -343,7 +346,6 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     for (int w = 0; w < W; ++w) lsc[w] = 0.0;
     int prev = -1;
     bool ok = true;
-    uint32_t phase = 0;
     for (int q = 0; q < cnt; ++q) {
         const int b = q & 1;
         const NodeJob nj = nodes[q];
@@ -538,6 +540,27 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) 
     }
 }
 
+template <class T, int R, int MINB, int W, int RB>
+__global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) {
+    uint32_t phase = 0;
+    prune_tile<T, R, MINB, W, RB>(a, a.tile_begin + blockIdx.x, phase, true);
+}
+
+// Persistent form: one wave of CTAs (the SMs times the CTAs each holds) walks
+// the tiles in a grid-stride loop. The copy barriers are initialised once and
+// their phases carried from tile to tile; every copy a tile issues is waited
+// on inside that tile.
+template <class T, int R, int MINB, int W, int RB>
+__global__ void __launch_bounds__(32 * R, MINB) prune_kernel_persistent(const PruneArgs a, int ntiles) {
+    uint32_t phase = 0;
+    bool init = true;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        prune_tile<T, R, MINB, W, RB>(a, a.tile_begin + t, phase, init);
+        init = false;
+        __syncthreads();
+    }
+}
+
 __global__ void reduce_kernel(const int32_t* __restrict__ tile_off, const double* __restrict__ partial,
                               const PartHdr* __restrict__ hdr, int first, int count,
                               double* __restrict__ lnl, int* __restrict__ status) {
@@ -582,6 +605,21 @@ cudaError_t launch_pmat(const PmJob* mjobs, int n, const PJob* jobs, const PartH
 namespace {
 
 template <class T, int R, int MINB, int W, int RB>
+cudaError_t launch_prune_persistent_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
+    const size_t smem = sizeof(T) * 4 * (size_t)kPBlock * R;
+    auto k = prune_kernel_persistent<T, R, MINB, W, RB>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * R, smem)) != cudaSuccess) return e;
+    const int grid = std::max(1, std::min(ntiles, sms * std::max(per_sm, 1)));
+    k<<<grid, 32 * R, smem, st>>>(a, ntiles);
+    return cudaGetLastError();
+}
+
+template <class T, int R, int MINB, int W, int RB>
 cudaError_t launch_prune_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
     const size_t smem = sizeof(T) * 4 * (size_t)kPBlock * R;
     cudaError_t e = cudaFuncSetAttribute(prune_kernel<T, R, MINB, W, RB>,
@@ -599,9 +637,11 @@ cudaError_t launch_prune_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
 //           7 (1,4,2)  8 (1,3,2)
 //           FP32 only, where 40 registers hold a lane's two 20-vectors:
 //           9 (1,5,1)  10 (1,6,1)  11 (1,5,4)
+//           persistent (one wave, grid-stride over tiles): FP64 9 (1,3,4),
+//           FP32 12 (1,4,4)
 //   other:  0 (1,-,1)  1 (1,-,4)  2 (2,-,1)
 // W = 2 variants take 64-slot tiles, the others 32-slot tiles.
-int simt_variants(int R, bool fp32) { return R == 4 ? (fp32 ? 12 : 9) : 3; }
+int simt_variants(int R, bool fp32) { return R == 4 ? (fp32 ? 13 : 10) : 3; }
 int simt_width(int R, int v) { return (R == 4 ? v == 6 : v == 2) ? 2 : 1; }
 
 template <class T, int R, int MINB, int MINB2>
@@ -624,6 +664,7 @@ cudaError_t launch_prune_r4(const PruneArgs& a, int ntiles, int variant, cudaStr
         case 6: return launch_prune_t<T, 4, 2, 2, 1>(a, ntiles, st);
         case 7: return launch_prune_t<T, 4, 4, 1, 2>(a, ntiles, st);
         case 8: return launch_prune_t<T, 4, 3, 1, 2>(a, ntiles, st);
+        case 9: return launch_prune_persistent_t<T, 4, 3, 1, 4>(a, ntiles, st);
         default: return launch_prune_t<T, 4, 4, 1, 1>(a, ntiles, st);
     }
 }
@@ -649,6 +690,7 @@ cudaError_t launch_prune_fp32(const PruneArgs& a, int ntiles, int variant, cudaS
             case 9: return launch_prune_t<float, 4, 5, 1, 1>(a, ntiles, st);
             case 10: return launch_prune_t<float, 4, 6, 1, 1>(a, ntiles, st);
             case 11: return launch_prune_t<float, 4, 5, 1, 4>(a, ntiles, st);
+            case 12: return launch_prune_persistent_t<float, 4, 4, 1, 4>(a, ntiles, st);
             default: break;
         }
     }

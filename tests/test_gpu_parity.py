@@ -391,3 +391,39 @@ def test_every_fp32_variant_matches_oracle(cfg):
         for i in range(cfg.particles):
             assert abs(got[i] - refs[i]) <= MIXED_ATOL, (v, i, got[i] - refs[i])
     eng.close()
+
+
+@pytest.mark.parametrize("precision", [smccat.PREC_FP64, smccat.PREC_FP32], ids=["fp64", "fp32"])
+def test_persistent_variant_over_many_tiles(precision):
+    """The persistent pruning variant (one wave of CTAs walking ~1,000 tiles,
+    several per CTA) gives the same values as the one-tile-per-CTA kernel it
+    wraps, on full refreshes and on lockstep rejuvenation with finished
+    (inactive) particles."""
+    cfg = workload.WorkloadConfig("many_tiles", T=12, S=2000, R=4, particles=16, iterations=1,
+                                  lg=False, invar=True, cat=False, alpha=0.5, pinv=0.1, seed=21)
+    rng = np.random.default_rng(cfg.seed)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    st = workload.make_particles(cfg, cfg.particles, rng)
+    fp32 = precision == smccat.PREC_FP32
+    base_v, pers_v = (4, 12) if fp32 else (3, 9)
+    outs = []
+    for v in (base_v, pers_v):
+        eng = smccat.Engine(codes, cfg.R, cfg.particles, max_classes=st["logits"].shape[1],
+                            lg=cfg.lg, invar=cfg.invar, cat=cfg.cat, precision=precision)
+        eng.set_kernel_variant(v)
+        eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                          st["logits"], st["assign"], st["pinv"], st["shape"])
+        eng.refresh(full=True)
+        full = eng.lnl()
+        eng.rejuvenate(iterations=2, temperature=0.8, seed=5)
+        outs.append((full, eng.lnl(), eng.get_particles()))
+        eng.close()
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    fin = outs[1][2]
+    for i in range(0, cfg.particles, 5):
+        ref, _ = oracle_lnl(codes, fin, i, cfg.R)
+        if fp32:
+            assert abs(outs[1][1][i] - ref) <= MIXED_ATOL
+        else:
+            assert outs[1][1][i] == pytest.approx(ref, rel=RTOL)
