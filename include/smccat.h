@@ -452,10 +452,12 @@ typedef struct smccat_profile {
  * particles must have no pending edits; their likelihoods are recomputed. */
 int smccat_autotune(smccat_ctx* ctx, int32_t reps, int32_t* variant_out, double* ms_out);
 
-/* Number of pruning-kernel variants of this context (SIMT kernels of several
- * schedules and register caps; FP64 contexts then add FP64 tensor-path
- * kernels), the one in use, and a way to pin one (what smccat_autotune
- * sets). A new context starts on the variant measured fastest on B200. */
+/* Number of pruning-kernel variants of this context, the one in use, and a
+ * way to pin one (what smccat_autotune sets). The variants are SIMT kernels
+ * of several schedules and register caps, persistent forms of the fastest of
+ * them at four rate categories, then the FP64 tensor-path kernels (FP64
+ * contexts) or the tcgen05 3xTF32 kernel on 128-slot tiles (FP32 contexts).
+ * A new context starts on the variant measured fastest on B200. */
 int smccat_kernel_variants(smccat_ctx* ctx, int32_t* count, int32_t* current);
 int smccat_set_kernel_variant(smccat_ctx* ctx, int32_t variant);
 
