@@ -193,10 +193,9 @@ def dgemm_peak_tflops():
 def cpu_baseline(cfg, codes, st, n_sample, min_seconds=10.0):
     """Time the oracle's OpenMP full refresh on a bounded particle sample."""
     import oracle
-    from smccat import discretize_gamma
     n = min(n_sample, st["parent"].shape[0])
     sl = slice(0, n)
-    rates = np.stack([discretize_gamma(s, cfg.R) for s in st["shape"][sl]])
+    rates = np.stack([oracle.discretize_gamma(s, cfg.R) for s in st["shape"][sl]])
     args = (codes, st["parent"][sl], st["branch"][sl], st["base"][sl], st["num_classes"][sl],
             st["logits"][sl], st["assign"][sl], st["pinv"][sl], rates)
     threads = oracle.max_threads()
@@ -211,7 +210,8 @@ def cpu_baseline(cfg, codes, st, n_sample, min_seconds=10.0):
     units = reps * n * cfg.S * cfg.R
     return {"value": units / el, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{n} particles x {cfg.S} sites x {cfg.R} categories, full refresh, "
-                      f"{reps} repetitions in {el:.1f} s (FP64 oracle, OpenMP over particles)"}
+                      f"{reps} repetitions in {el:.1f} s: the oracle's speed (FP64 C++ "
+                      "restatement of the reference's path, OpenMP over particles)"}
 
 
 def measure_reassignment(codes, st, cfg, n, local, torch):
@@ -436,18 +436,44 @@ def measure_config_waves(cid, steps, local, rank, particles=0, oracle_sample=2, 
     return res
 
 
+def cl_bytes(cfg, n, w=8):
+    """Device bytes of the partial-likelihood buffers of n particles: T-1
+    internal nodes x 2 workspaces x 20 states x R x sites padded to 32."""
+    spad = (cfg.S + 31) // 32 * 32
+    return (cfg.T - 1) * 2 * 20 * cfg.R * spad * w * n
+
+
+MODEL_NAMES = {"lg_g4_16x500": "LG+G4", "gtr_g4_i_48x2000": "GTR+G4+I",
+               "cat_gtr_g4_64x5000": "CAT-GTR+G4", "cat_uneven_100x10000": "CAT-GTR+G4, K ~ U{8..120}",
+               "cat_gtr_g4_i_128x20000": "CAT-GTR+G4+I"}
+
+
+def bench_config(cfg, n, world):
+    """The workload description both arms print, identical between them."""
+    return {"workload": cfg.name, "taxa": cfg.T, "sites": cfg.S, "rates": cfg.R,
+            "particles_per_gpu": n,
+            "model": MODEL_NAMES.get(cfg.name, cfg.name),
+            "step": "full refresh of every particle (refreshLikelihood(true))",
+            "l2": "inputs larger than L2 (partials %.1f GB per GPU at FP64)" % (cl_bytes(cfg, n) / 1e9),
+            "parallelism": f"particles sharded, {world} GPU(s), no collective"}
+
+
 def run_reference(args, rank, world):
-    """Reference arm: the CPU implementation of the path on the host cores."""
+    """Reference arm: the CPU implementation of the path on the host cores,
+    over the same particles as the GPU arm's rank 0. The inputs are built with
+    the oracle's gamma discretisation and LG table, so this process never
+    loads the engine library."""
     if rank != 0:
         return
     import oracle
-    from smccat import discretize_gamma, workload
+    from smccat import workload
     cfg = workload.CONFIGS[args.config]
-    rng = np.random.default_rng(cfg.seed)
-    codes, _ = workload.simulate_alignment(cfg, rng)
-    n = min(args.cpu_sample, cfg.particles)
-    st = workload.make_particles(cfg, n, rng)
-    rates = np.stack([discretize_gamma(s, cfg.R) for s in st["shape"]])
+    codes, _ = workload.simulate_alignment(cfg, np.random.default_rng(cfg.seed),
+                                           gamma_fn=oracle.discretize_gamma, lg_fn=oracle.lg_base)
+    n = args.particles or cfg.particles
+    st = workload.make_particles(cfg, n, np.random.default_rng(cfg.seed * 1000),
+                                 lg_fn=oracle.lg_base)
+    rates = np.stack([oracle.discretize_gamma(s, cfg.R) for s in st["shape"]])
     a = (codes, st["parent"], st["branch"], st["base"], st["num_classes"], st["logits"],
          st["assign"], st["pinv"], rates)
     threads = oracle.max_threads()
@@ -463,12 +489,13 @@ def run_reference(args, rank, world):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": cfg.name, "taxa": cfg.T, "sites": cfg.S, "rates": cfg.R,
-                   "particles_per_step": n, "model": "GTR+G4+I" if args.config == 2 else cfg.name},
+        "config": bench_config(cfg, n, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{n} particles x {cfg.S} sites x {cfg.R} categories per step "
-                                   "(FP64 oracle restating the reference's refreshLikelihood(true), "
-                                   "OpenMP over particles)"},
+                         "sample": f"all {n} particles x {cfg.S} sites x {cfg.R} categories per "
+                                   "step: the oracle's speed (an FP64 C++ restatement of the "
+                                   "reference's refreshLikelihood(true) with its OpenMP loop over "
+                                   "particles; the reference itself needs Eigen and Boost, absent "
+                                   "here)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -728,12 +755,8 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": cfg.name, "taxa": cfg.T, "sites": cfg.S, "rates": cfg.R,
-                       "particles_per_gpu": n, "model": "GTR+G4+I" if args.config == 2 else cfg.name,
-                       "step": "full refresh of every particle (refreshLikelihood(true))",
-                       "l2": "inputs larger than L2 (CL buffers %.1f GB per GPU)" % (eng.device_bytes / 1e9),
-                       "parallelism": f"particles sharded, {world} GPU(s), no collective",
-                       "autotune": tuned},
+            "config": bench_config(cfg, n, world),
+            "autotune": tuned,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": prof_e2e["h2d_bytes"] // args.steps,
                     "d2h_bytes_per_step": prof_e2e["d2h_bytes"] // args.steps},

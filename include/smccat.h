@@ -111,11 +111,15 @@ int smccat_lg_exchangeabilities(double* out190);
  *   p_out   [num_classes][num_times][20][20]  row-major P(t) (device)
  * num_classes may be at most 512; larger requests return SMCCAT_EINVAL. Work
  * is queued on `stream` (a cudaStream_t, NULL = legacy default stream) on the
- * current device and the call returns without waiting. The first call on a
- * device resolves the array's device address (one-time set-up, done with that
- * device current); make that first call before any stream capture. Every call
- * reuses the same array, so calls whose work overlaps on the GPU (e.g. on two
- * streams at once) race; order them on one stream. */
+ * current device and the call returns without waiting. Set-up: a call outside
+ * stream capture resolves the array's device address in the CUDA context
+ * current at the call (the device's primary context, or a context the host
+ * made current itself); a call under stream capture uses the address recorded
+ * by that context's last call outside capture, so make one call in each
+ * context before capturing (else SMCCAT_ESTATE). Launch errors are reported
+ * without clearing the runtime's last-error state. Every call reuses the same
+ * array, so calls whose work overlaps on the GPU (e.g. on two streams at once)
+ * race; order them on one stream. */
 int smccat_transition_matrices_noalloc(int32_t num_classes, const double* base,
                                        const double* logits, int32_t num_times,
                                        const double* times, double* p_out, void* stream);
@@ -460,6 +464,16 @@ int smccat_autotune(smccat_ctx* ctx, int32_t reps, int32_t* variant_out, double*
  * A new context starts on the variant measured fastest on B200. */
 int smccat_kernel_variants(smccat_ctx* ctx, int32_t* count, int32_t* current);
 int smccat_set_kernel_variant(smccat_ctx* ctx, int32_t variant);
+
+/* Polls a pruning kernel's bounded device waits (for its staged transition
+ * matrices, or its tensor-core products) make before giving up; polls < 0
+ * restores the default (4,194,304). A wait that gives up makes the refresh
+ * return SMCCAT_ETIMEOUT with NaN likelihoods, after the kernel has drained
+ * the copies it had in flight; the next refresh with a sufficient limit is
+ * unaffected. 0 makes every wait give up at once, which exercises that path
+ * without stalling or faulting the device. No counterpart in the reference
+ * (it has no device code). */
+int smccat_set_wait_limit(smccat_ctx* ctx, int32_t polls);
 
 /* Enable (1) or disable (0) per-launch CUDA-event timing; resets counters. */
 int smccat_set_profiling(smccat_ctx* ctx, int32_t enable);

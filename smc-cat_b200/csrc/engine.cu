@@ -84,6 +84,7 @@ struct smccat_ctx {
     size_t plan_cap = 0;
     int tile_cap = 0;
     int prune_variant = 0;      // chosen by smccat_autotune
+    uint32_t wait_limit = kDrainPolls;  // polls per bounded device wait (smccat_set_wait_limit)
     int tile_sites = kTileSites;  // slots per pruning tile, as the variant expects
 
     std::vector<uint8_t> codes;
@@ -770,6 +771,7 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
     a.site_lnl = c->d_site_lnl;
     a.partial = c->d_partial;
     a.status = c->d_status;
+    a.wait_limit = c->wait_limit;
     const int ntiles = c->tile_off[first + count] - c->tile_off[first];
     if (ntiles > 0)
         CK(launch(c, SMCCAT_KERNEL_PRUNE,
@@ -852,6 +854,7 @@ int smccat::device_view(smccat_ctx* c, int first, int count, DeviceView* v) {
     a.site_lnl = c->d_site_lnl;
     a.partial = c->d_partial;
     a.status = c->d_status;
+    a.wait_limit = c->wait_limit;
     v->ntiles = c->tile_off[first + count] - c->tile_off[first];
     v->variant = c->prune_variant;
     v->lnl = c->d_lnl;
@@ -1110,6 +1113,12 @@ int smccat_set_kernel_variant(smccat_ctx* c, int32_t variant) {
     if (variant < 0 || variant >= prune_variants(c->d.R, c->esz == 4))
         return fail(SMCCAT_EINVAL, "kernel variant out of range");
     select_variant(c, variant);
+    return SMCCAT_OK;
+}
+
+int smccat_set_wait_limit(smccat_ctx* c, int32_t polls) {
+    if (!c) return fail(SMCCAT_EINVAL, "null context");
+    c->wait_limit = polls < 0 ? kDrainPolls : static_cast<uint32_t>(polls);
     return SMCCAT_OK;
 }
 

@@ -6,6 +6,11 @@
 
 namespace smccat {
 
+// mbarrier polls before a bounded device wait gives up (a pruning kernel's
+// wait for its staged transition matrices or tensor-core products), and the
+// polls a kernel then spends draining the copies it still has in flight.
+constexpr uint32_t kDrainPolls = 1u << 22;
+
 struct Dims {
     int T, S, Spad, R, N, NI, Kmax;
 };
@@ -32,6 +37,7 @@ struct PruneArgs {
     double* site_lnl;
     double* partial;
     int* status;      // bit 1: NaN likelihood, bit 2: a bounded wait gave up
+    uint32_t wait_limit;  // polls per bounded wait (kDrainPolls unless a test lowers it)
 };
 
 cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d, cudaStream_t st);

@@ -30,7 +30,6 @@ namespace smccat {
 
 namespace {
 
-constexpr uint32_t kWaitLimit = 1u << 22;  // mbarrier polls before giving up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -76,9 +75,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Wait for phase `parity` of `bar` to complete; false after kWaitLimit polls.
-__device__ __noinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
+// Wait for phase `parity` of `bar` to complete; false after `limit` polls.
+__device__ __noinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -275,8 +274,13 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
 // reduction are FP64 in both.
 // One tile. `phase` holds each P buffer's next barrier parity; the barriers
 // are initialised when `init` is set (a CTA's first tile) and reused after.
+// Bounded waits: once a wait gives up (a.wait_limit polls), the warp issues no
+// further copies, and lane 0 -- the lane that issued them -- drains every copy
+// still in flight (waiting on its un-toggled parity, with the full limit)
+// before the buffers are reused. Returns false, uniformly across the CTA,
+// when any warp gave up.
 template <class T, int R, int MINB, int W, int RB>
-__device__ __forceinline__ void prune_tile(const PruneArgs& a, const int tile_id, uint32_t& phase, bool init) {
+__device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id, uint32_t& phase, bool init) {
     const Dims d = a.d;
     const Tile tl = a.tiles[tile_id];
     const int p = tl.p;
@@ -328,16 +332,18 @@ __device__ __forceinline__ void prune_tile(const PruneArgs& a, const int tile_id
         fence_mbar_init();
     }
     __syncthreads();
-    if (!h->active) return;  // uniform across the CTA (after the barriers exist)
+    if (!h->active) return true;  // uniform across the CTA (after the barriers exist)
 
     const int cnt = h->node_cnt;
     const NodeJob* nodes = a.nodes + h->node_off;
+    uint32_t pend = 0;  // lane 0: bit b set while a copy into buffer b is not yet waited on
     if (cnt > 0 && lane == 0) {
         fence_proxy_async();  // a previous tile's root rows were written here
         const NodeJob nj = nodes[0];
         mbar_expect_tx(&bars[r][0], 2 * kPBytes);
         tma_load_1d(buf, pblock(nj.c1, (nj.ws >> 3) & 1), kPBytes, &bars[r][0]);
         tma_load_1d(buf + kPBlock, pblock(nj.c2, (nj.ws >> 4) & 1), kPBytes, &bars[r][0]);
+        pend = 1u;
     }
 
     T y[W][kStates];
@@ -349,7 +355,7 @@ __device__ __forceinline__ void prune_tile(const PruneArgs& a, const int tile_id
     for (int q = 0; q < cnt; ++q) {
         const int b = q & 1;
         const NodeJob nj = nodes[q];
-        if (q + 1 < cnt && lane == 0) {
+        if (ok && q + 1 < cnt && lane == 0) {
             // Buffer b^1 was last read at node q-1 (the warp synchronised after it).
             const NodeJob nx = nodes[q + 1];
             fence_proxy_async();
@@ -358,6 +364,7 @@ __device__ __forceinline__ void prune_tile(const PruneArgs& a, const int tile_id
                         &bars[r][b ^ 1]);
             tma_load_1d(buf + (b ^ 1) * 2 * kPBlock + kPBlock, pblock(nx.c2, (nx.ws >> 4) & 1),
                         kPBytes, &bars[r][b ^ 1]);
+            pend |= 1u << (b ^ 1);
         }
         // Roles: the child computed just before (if any) is in registers; the
         // other child is a tip (gather) or a stored partial (load).
@@ -381,11 +388,15 @@ __device__ __forceinline__ void prune_tile(const PruneArgs& a, const int tile_id
                 for (int w = 0; w < W; ++w) code_o[w] = cp[site[w]];
             }
         }
-        if (ok && !mbar_wait_bounded(&bars[r][b], (phase >> b) & 1)) {
-            ok = false;
-            atomicOr(a.status, 2);
+        if (ok) {
+            if (mbar_wait_bounded(&bars[r][b], (phase >> b) & 1, a.wait_limit)) {
+                phase ^= 1u << b;
+                pend &= ~(1u << b);
+            } else {
+                ok = false;
+                atomicOr(a.status, 2);
+            }
         }
-        phase ^= 1u << b;
         if (ok && valid) {
             const T* Pf = buf + (size_t)(b * 2 + fi) * kPBlock;
             const T* Po = buf + (size_t)(b * 2 + oi) * kPBlock;
@@ -470,13 +481,17 @@ __device__ __forceinline__ void prune_tile(const PruneArgs& a, const int tile_id
         prev = nj.node;
         __syncwarp();
     }
-    if (!ok) {
-        // Let any copy still in flight land before the CTA's shared memory is released.
-        if (lane == 0) {
-            mbar_wait_bounded(&bars[r][0], phase & 1);
-            mbar_wait_bounded(&bars[r][1], (phase >> 1) & 1);
-        }
-        bad = 1;
+    if (!ok) bad = 1;
+    // Let every copy lane 0 issued and never waited on land before the warp's
+    // buffers are reused (the root rows below) or the CTA exits. Each such
+    // copy's phase is the un-toggled parity of its buffer.
+    if (lane == 0 && pend) {
+#pragma unroll
+        for (int bb = 0; bb < 2; ++bb)
+            if ((pend >> bb) & 1u) {
+                if (mbar_wait_bounded(&bars[r][bb], (phase >> bb) & 1, kDrainPolls)) phase ^= 1u << bb;
+                else bad = 1;
+            }
     }
     __syncwarp();  // the warp's buffers are free from here on (red(r) reuses them)
     // Root reduction for this tile.
@@ -503,6 +518,7 @@ __device__ __forceinline__ void prune_tile(const PruneArgs& a, const int tile_id
         }
     }
     __syncthreads();
+    const bool tile_ok = bad == 0;  // read by every thread between the same two barriers
     if (r == 0) {
         double v = 0.0;
 #pragma unroll
@@ -538,6 +554,7 @@ __device__ __forceinline__ void prune_tile(const PruneArgs& a, const int tile_id
         v = warp_sum(v);
         if (lane == 0) a.partial[tile_id] = v;
     }
+    return tile_ok;
 }
 
 template <class T, int R, int MINB, int W, int RB>
@@ -555,9 +572,10 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_kernel_persistent(const Pr
     uint32_t phase = 0;
     bool init = true;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        prune_tile<T, R, MINB, W, RB>(a, a.tile_begin + t, phase, init);
+        const bool ok = prune_tile<T, R, MINB, W, RB>(a, a.tile_begin + t, phase, init);
         init = false;
         __syncthreads();
+        if (!ok) break;  // a wait gave up: the CTA's remaining tiles stay unevaluated (status bit 2)
     }
 }
 

@@ -21,7 +21,6 @@
 namespace smccat {
 namespace {
 
-constexpr uint32_t kWaitLimitD = 1u << 22;
 constexpr uint32_t kPBytesD = kPBlock * sizeof(double);
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -52,8 +51,8 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
         : "memory");
 }
 
-__device__ __noinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitLimitD; ++i) {
+__device__ __noinline__ bool bar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -138,11 +137,13 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_dmma_kernel(const PruneArg
     __syncthreads();
     const int cnt = h->node_cnt;
     const NodeJob* nodes = a.nodes + h->node_off;
+    uint32_t pend = 0;  // lane 0: bit b set while a copy into buffer b is not yet waited on
     if (cnt > 0 && lane == 0) {
         const NodeJob nj = nodes[0];
         bar_expect(&bars[r][0], 2 * kPBytesD);
         bulk_load(buf, pblock(nj.c1, (nj.ws >> 3) & 1), kPBytesD, &bars[r][0]);
         bulk_load(buf + kPBlock, pblock(nj.c2, (nj.ws >> 4) & 1), kPBytesD, &bars[r][0]);
+        pend = 1u;
     }
 
     double y[4][3][2];  // D layout of the last computed node
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_dmma_kernel(const PruneArg
     for (int q = 0; q < cnt; ++q) {
         const int b = q & 1;
         const NodeJob nj = nodes[q];
-        if (q + 1 < cnt && lane == 0) {
+        if (ok && q + 1 < cnt && lane == 0) {  // no new copies once a wait has given up
             const NodeJob nx = nodes[q + 1];
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             bar_expect(&bars[r][b ^ 1], 2 * kPBytesD);
@@ -163,12 +164,17 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_dmma_kernel(const PruneArg
                       &bars[r][b ^ 1]);
             bulk_load(buf + (b ^ 1) * 2 * kPBlock + kPBlock, pblock(nx.c2, (nx.ws >> 4) & 1), kPBytesD,
                       &bars[r][b ^ 1]);
+            pend |= 1u << (b ^ 1);
         }
-        if (ok && !bar_wait(&bars[r][b], (phase >> b) & 1)) {
-            ok = false;
-            atomicOr(a.status, 2);
+        if (ok) {
+            if (bar_wait(&bars[r][b], (phase >> b) & 1, a.wait_limit)) {
+                phase ^= 1u << b;
+                pend &= ~(1u << b);
+            } else {
+                ok = false;
+                atomicOr(a.status, 2);
+            }
         }
-        phase ^= 1u << b;
         if (ok) {
             const bool c1prev = nj.c1 == prev, c2prev = nj.c2 == prev;
             const int oi = c1prev ? 1 : 0;
@@ -297,12 +303,12 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_dmma_kernel(const PruneArg
         prev = nj.node;
         __syncwarp();
     }
-    if (!ok) {
-        if (lane == 0) {
-            bar_wait(&bars[r][0], phase & 1);
-            bar_wait(&bars[r][1], (phase >> 1) & 1);
-        }
-        bad = 1;
+    if (!ok) bad = 1;
+    // Lane 0 drains every copy it issued and never waited on (each on its
+    // buffer's un-toggled parity) before the CTA's shared memory is released.
+    if (lane == 0 && pend) {
+        for (int bb = 0; bb < 2; ++bb)
+            if (((pend >> bb) & 1u) && !bar_wait(&bars[r][bb], (phase >> bb) & 1, kDrainPolls)) bad = 1;
     }
     // ---- root reduction
     if (cnt == 0) {

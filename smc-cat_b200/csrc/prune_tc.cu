@@ -40,7 +40,6 @@ constexpr uint32_t kCoreLbo = 128;                 // next core matrix along K
 constexpr uint32_t kCoreSbo = (kTcPad / 4) * 128;  // next 8-row group
 constexpr uint32_t kBBytes = kTcPad * kTcPad * 4;  // one B operand tile
 constexpr uint32_t kPBytesF = kPBlock * sizeof(float);
-constexpr uint32_t kWaitLimitTc = 1u << 22;
 // idesc: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), K-major
 // A and B, N >> 3 at bit 17, M >> 4 at bit 24.
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcPad >> 3) << 17) |
@@ -84,8 +83,8 @@ __device__ __forceinline__ void tc_bulk(void* dst, const void* src, uint32_t byt
         : "memory");
 }
 
-__device__ __noinline__ bool tc_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitLimitTc; ++i) {
+__device__ __noinline__ bool tc_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -195,7 +194,16 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
         tc_bulk(dst, pblock(nj.c1, (nj.ws >> 3) & 1, r), kPBytesF, &bars[f & 1]);
         tc_bulk(dst + kPBlock, pblock(nj.c2, (nj.ws >> 4) & 1, r), kPBytesF, &bars[f & 1]);
     };
-    if (tid == 0 && nsteps > 0) issue(0);
+    // Thread 0 issues every copy and product. It tracks which are still in
+    // flight (copy buffers in `pend`, the last product commit in `mma_pend`),
+    // stops issuing once a wait has given up, and drains the rest before the
+    // CTA releases its shared and tensor memory.
+    uint32_t pend = 0;
+    bool mma_pend = false;
+    if (tid == 0 && nsteps > 0) {
+        issue(0);
+        pend = 1u;
+    }
 
     bool ok = true;
     uint32_t tphase = 0, mphase = 0;
@@ -211,9 +219,10 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
             const int f = r * cnt + q;
             const int b = f & 1;
             const NodeJob nj = nodes[q];
-            if (tid == 0 && f + 1 < nsteps) {
+            if (tid == 0 && ok && f + 1 < nsteps) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 issue(f + 1);  // buffer b ^ 1 was last read at step f - 1 (synchronised since)
+                pend |= 1u << (b ^ 1);
             }
             // The child computed just before (if any) is in registers; the
             // other is a tip (column of P) or a stored partial.
@@ -221,11 +230,15 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
             const int oi = c1prev ? 1 : 0;
             const int fi = 1 - oi;
             const bool has_prev = c1prev || c2prev;
-            if (ok && !tc_wait(&bars[b], (tphase >> b) & 1)) {
-                ok = false;
-                if (tid == 0) atomicOr(a.status, 2);
+            if (ok) {
+                if (tc_wait(&bars[b], (tphase >> b) & 1, a.wait_limit)) {
+                    tphase ^= 1u << b;
+                    pend &= ~(1u << b);
+                } else {
+                    ok = false;
+                    atomicOr(a.status, 2);
+                }
             }
-            tphase ^= 1u << b;
             const float* Pst = pbuf + (size_t)b * 2 * kPBlock;
             // B operands (P hi / lo) of the internal children.
             for (int ci = 0; ci < 2; ++ci) {
@@ -288,8 +301,8 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
                     }
                     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
                     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                    __syncthreads();
-                    if (tid == 0) {
+                    ok = __syncthreads_and(ok);  // one decision for the whole CTA
+                    if (tid == 0 && ok) {
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                         const uint32_t bh = sa(bop + (2 * ci) * kBBytes), bl = sa(bop + (2 * ci + 1) * kBBytes);
 #pragma unroll
@@ -304,12 +317,17 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
                         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                          sa(&mma_bar))
                                      : "memory");
+                        mma_pend = true;
                     }
-                    if (ok && !tc_wait(&mma_bar, mphase)) {
-                        ok = false;
-                        if (tid == 0) atomicOr(a.status, 2);
+                    if (ok) {
+                        if (tc_wait(&mma_bar, mphase, a.wait_limit)) {
+                            mphase ^= 1u;
+                            mma_pend = false;
+                        } else {
+                            ok = false;
+                            atomicOr(a.status, 2);
+                        }
                     }
-                    mphase ^= 1u;
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     uint32_t dv[kTcPad];
 #pragma unroll
@@ -366,15 +384,13 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
         for (int i = 0; i < kStates; ++i) s = fma(pi[i], (double)y[i], s);
         red[r * kTcSites + tid] = log(s) + lsc;
     }
-    if (!ok) {
-        bad = 1;
-        // Let copies and products still in flight land before the CTA's
-        // shared and tensor memory are released.
-        if (tid == 0) {
-            for (int x = 0; x < 2; ++x)
-                if (nsteps > x) tc_wait(&bars[x], ((tphase >> x) & 1) ^ 1);
-            tc_wait(&mma_bar, mphase ^ 1);
-        }
+    if (!ok) bad = 1;
+    // Let copies and products still in flight land (each on its un-toggled
+    // parity) before the CTA's shared and tensor memory are released.
+    if (tid == 0) {
+        for (int x = 0; x < 2; ++x)
+            if (((pend >> x) & 1u) && !tc_wait(&bars[x], (tphase >> x) & 1, kDrainPolls)) bad = 1;
+        if (mma_pend && !tc_wait(&mma_bar, mphase, kDrainPolls)) bad = 1;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

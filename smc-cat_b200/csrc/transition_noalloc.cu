@@ -12,10 +12,13 @@
 //
 // The array holds kNoAllocMaxClasses records (3.5 MB). Every GPU on which the
 // library's kernels get loaded keeps it until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "smccat.h"
 #include "spectral.cuh"
@@ -24,16 +27,36 @@ namespace smccat {
 namespace {
 
 constexpr int kNoAllocMaxClasses = 512;
-constexpr int kMaxDevices = 64;
+constexpr size_t kMaxContexts = 64;
 
 // Scratch for the spectral records of one call. Its contents persist from
 // call to call; every record a call reads is written earlier in that call.
 static __device__ __align__(256) double g_noalloc_spec[kNoAllocMaxClasses * kSpecStride];
 
-// Device address of g_noalloc_spec, per device ordinal (host code must not use
-// the symbol itself: on the host it names a stand-in, not device memory).
-double* g_noalloc_ptr[kMaxDevices] = {};
+// Device address of g_noalloc_spec per CUDA context (host code must not use
+// the symbol itself: on the host it names a stand-in, not device memory). The
+// key is the context current at the call, not the device ordinal: a host may
+// run this library under a context of its own (not the device's primary one),
+// and a context destroyed and re-created (cudaDeviceReset) gets the array at a
+// new address. A call outside stream capture resolves the address afresh and
+// records it; a call under capture, where resolving could trigger module
+// loading, uses the address recorded for its context.
+std::vector<std::pair<CUcontext, double*>> g_noalloc_ptr;
 std::mutex g_noalloc_mu;
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(f);
+    });
+    return fn;
+}
 
 __global__ void __launch_bounds__(32) noalloc_spec_kernel(const double* __restrict__ base,
                                                           const double* __restrict__ logits,
@@ -93,31 +116,51 @@ int smccat_transition_matrices_noalloc(int32_t num_classes, const double* base,
                                                std::to_string(num_classes));
     if (num_times < 1 || (long long)num_classes * num_times > 0x7fffffffLL)
         return noalloc_fail(SMCCAT_EINVAL, "num_times must be >= 1 and num_classes * num_times < 2^31");
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cap);
     if (e != cudaSuccess) return noalloc_fail(SMCCAT_ECUDA, cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(SMCCAT_ENODEV, "device ordinal out of range");
+    void* fresh = nullptr;
+    if (cap == cudaStreamCaptureStatusNone) {
+        // Set-up with the caller's context current (the runtime makes the
+        // device's primary context current if none is): resolve the device
+        // address of the scratch array in this context.
+        e = cudaGetSymbolAddress(&fresh, g_noalloc_spec);
+        if (e != cudaSuccess || !fresh)
+            return noalloc_fail(SMCCAT_ECUDA, std::string("cudaGetSymbolAddress: ") +
+                                                  cudaGetErrorString(e));
+    }
+    CtxGetCurrentFn get_ctx = ctx_get_current();
+    CUcontext ctx = nullptr;
+    if (!get_ctx || get_ctx(&ctx) != CUDA_SUCCESS || !ctx)
+        return noalloc_fail(SMCCAT_ECUDA, "no current CUDA context");
     double* scratch = nullptr;
     {
-        // One-time set-up per device, with that device current: resolve the
-        // device address of the scratch array.
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void* ptr = nullptr;
-            e = cudaGetSymbolAddress(&ptr, g_noalloc_spec);
-            if (e != cudaSuccess || !ptr)
-                return noalloc_fail(SMCCAT_ECUDA, std::string("cudaGetSymbolAddress: ") +
-                                                      cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = static_cast<double*>(ptr);
+        auto it = g_noalloc_ptr.begin();
+        while (it != g_noalloc_ptr.end() && it->first != ctx) ++it;
+        if (fresh) {
+            if (it != g_noalloc_ptr.end()) {
+                it->second = static_cast<double*>(fresh);
+            } else {
+                if (g_noalloc_ptr.size() >= kMaxContexts) g_noalloc_ptr.erase(g_noalloc_ptr.begin());
+                g_noalloc_ptr.emplace_back(ctx, static_cast<double*>(fresh));
+            }
+            scratch = static_cast<double*>(fresh);
+        } else {
+            if (it == g_noalloc_ptr.end())
+                return noalloc_fail(SMCCAT_ESTATE,
+                                    "first call in this CUDA context must come before stream capture");
+            scratch = it->second;
         }
-        scratch = g_noalloc_ptr[dev];
     }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Launch errors are peeked, not cleared: the error state belongs to the host
+    // program as much as to this call.
     noalloc_spec_kernel<<<num_classes, 32, 0, st>>>(base, logits, scratch);
-    e = cudaGetLastError();
+    e = cudaPeekAtLastError();
     if (e != cudaSuccess) return noalloc_fail(SMCCAT_ECUDA, cudaGetErrorString(e));
     noalloc_pmat_kernel<<<num_classes * num_times, 128, 0, st>>>(scratch, num_times, times, p_out);
-    e = cudaGetLastError();
+    e = cudaPeekAtLastError();
     if (e != cudaSuccess) return noalloc_fail(SMCCAT_ECUDA, cudaGetErrorString(e));
     return SMCCAT_OK;
 }

@@ -17,7 +17,7 @@ _PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(_PKG_DIR, "lib", "libsmccat.so")
 HEADER_PATH = os.path.join(os.path.dirname(_PKG_DIR), "include", "smccat.h")
 
-OK, EINVAL, ECUDA, ENOMEM, ESTATE, ENUMERIC, ENODEV = range(7)
+OK, EINVAL, ECUDA, ENOMEM, ESTATE, ENUMERIC, ENODEV, ETIMEOUT = range(8)
 MODEL_LG, MODEL_INVAR, MODEL_CAT, MODEL_PATTERNS = 1, 2, 4, 8
 PREC_FP64, PREC_FP32 = 0, 1
 REFRESH_DIRTY, REFRESH_FULL = 0, 1
@@ -125,6 +125,7 @@ def lib():
         "smccat_autotune": ([vp, _i32, _ip, _dp], ctypes.c_int),
         "smccat_kernel_variants": ([vp, _ip, _ip], ctypes.c_int),
         "smccat_set_kernel_variant": ([vp, _i32], ctypes.c_int),
+        "smccat_set_wait_limit": ([vp, _i32], ctypes.c_int),
         "smccat_set_tuning": ([vp, ctypes.POINTER(Tuning)], ctypes.c_int),
         "smccat_get_tuning": ([vp, ctypes.POINTER(Tuning)], ctypes.c_int),
         "smccat_set_rate_cholesky": ([vp, _dp], ctypes.c_int),
@@ -506,6 +507,10 @@ class Engine:
 
     def set_kernel_variant(self, v: int):
         _check(lib().smccat_set_kernel_variant(self._h, int(v)))
+
+    def set_wait_limit(self, polls: int):
+        """Polls per bounded device wait; a negative value restores the default."""
+        _check(lib().smccat_set_wait_limit(self._h, int(polls)))
 
     def set_profiling(self, enable: bool):
         _check(lib().smccat_set_profiling(self._h, 1 if enable else 0))

@@ -15,6 +15,11 @@ seed:
 Particle states follow the reference's initialisation (Particle.cpp:81-166):
 random tree, LG or N(0,1) exchangeabilities, 19 N(0,1) logits + 0 per class,
 pinv ~ U(0,1) with +I, shape ~ Gamma(3, 2) with R > 1.
+
+The gamma discretisation and the LG table come from the engine library by
+default. A caller that must not load it (the CPU timing of the reference's
+path) passes its own ``gamma_fn(shape, R)`` and ``lg_fn()``; the values are
+the same (both restate Miscellaneous.hpp:22-37 and RateMatrices.hpp:7-111).
 """
 from __future__ import annotations
 
@@ -22,7 +27,15 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import discretize_gamma, lg_exchangeabilities
+
+def _sources(gamma_fn, lg_fn):
+    """The gamma-discretisation and LG-table functions to use: the given ones,
+    else the engine library's (imported only when one is missing)."""
+    if gamma_fn is None or lg_fn is None:
+        from . import discretize_gamma, lg_exchangeabilities
+        gamma_fn = gamma_fn or discretize_gamma
+        lg_fn = lg_fn or lg_exchangeabilities
+    return gamma_fn, lg_fn
 
 
 @dataclass
@@ -140,8 +153,10 @@ def crp_assign(rng, S, concentration, max_classes=None):
     return assign, len(counts)
 
 
-def simulate_alignment(cfg: WorkloadConfig, rng: np.random.Generator | None = None):
+def simulate_alignment(cfg: WorkloadConfig, rng: np.random.Generator | None = None,
+                       gamma_fn=None, lg_fn=None):
     """Simulate (codes [T][S] uint8, truth dict) for a workload config."""
+    discretize_gamma, lg_exchangeabilities = _sources(gamma_fn, lg_fn)
     rng = np.random.default_rng(cfg.seed) if rng is None else rng
     T, S, R = cfg.T, cfg.S, cfg.R
     parent, branch = random_tree(rng, T)
@@ -191,8 +206,10 @@ def simulate_alignment(cfg: WorkloadConfig, rng: np.random.Generator | None = No
     return codes, truth
 
 
-def make_particles(cfg: WorkloadConfig, n: int, rng: np.random.Generator, kmax: int | None = None):
+def make_particles(cfg: WorkloadConfig, n: int, rng: np.random.Generator, kmax: int | None = None,
+                   lg_fn=None):
     """Particle states drawn like the reference's initialisation (packed arrays)."""
+    lg_exchangeabilities = _sources(None, lg_fn)[1] if cfg.lg else None
     T, S, R = cfg.T, cfg.S, cfg.R
     N = 2 * T - 1
     if cfg.cat:

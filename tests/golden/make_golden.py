@@ -18,24 +18,36 @@ third-party library does the work there:
 * Tip encoding / invariance (Particle.cpp:44-73), lnPrior (Particle.cpp:484-517)
   and computeNextStep (Miscellaneous.hpp:42-109).
 
-Run from the repository root:  python tests/golden/make_golden.py
-It needs the reference checkout only for the LG table; the fixtures it writes
-are committed so the tests never read the reference.
+Run from the repository root:
+    python tests/golden/make_golden.py <Smc-CAT checkout>
+(or with the checkout in the environment variable SMCCAT_REFERENCE). It needs
+the reference checkout only for the LG table, read from
+src/analysis/RateMatrices.hpp inside it; the fixtures it writes are committed
+so the tests never read the reference.
 """
 from __future__ import annotations
 
 import json
 import os
 import re
+import sys
 
 import numpy as np
 from scipy import stats
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/src/analysis/RateMatrices.hpp"
+LG_SOURCE = os.path.join("src", "analysis", "RateMatrices.hpp")
 
 
-def parse_lg(path=REF):
+def reference_root():
+    """The Smc-CAT checkout: the first argument, else $SMCCAT_REFERENCE."""
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SMCCAT_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py <Smc-CAT checkout>  (or set SMCCAT_REFERENCE)")
+    return root
+
+
+def parse_lg(path):
     txt = open(path).read()
     m = np.full((20, 20), np.nan)
     for i, j, v in re.findall(r"m\(\s*(\d+),\s*(\d+)\)\s*=\s*([0-9.]+);", txt):
@@ -236,7 +248,7 @@ def simulate_codes(rng, T, S, gap_frac=0.05, special=True):
 def main():
     rng = np.random.default_rng(20261203)
     out = {}
-    lg = parse_lg()
+    lg = parse_lg(os.path.join(reference_root(), LG_SOURCE))
     out["lg_base"] = lg.tolist()
 
     gam = []

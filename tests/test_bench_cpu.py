@@ -20,7 +20,7 @@ def test_reference_arm_under_two_ranks():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), "bench.py",
            "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3",
-           "--cpu-sample", "2"]
+           "--particles", "2"]
     out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
@@ -33,3 +33,26 @@ def test_reference_arm_under_two_ranks():
         assert key in rec
     assert rec["e2e"]["h2d_bytes_per_step"] == 0 and rec["e2e"]["d2h_bytes_per_step"] == 0
     assert rec["cpu_baseline"]["kind"] == "port"
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """The reference arm builds its inputs with the oracle's gamma
+    discretisation and LG table: the engine library never enters the process,
+    and its config is the GPU arm's."""
+    code = ("import runpy, sys, json\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0',"
+            " '--particles', '2']\n"
+            "runpy.run_path('bench.py', run_name='__main__')\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('LOADED', json.dumps({'engine': 'libsmccat' in maps, 'oracle': 'liboracle' in maps}))\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    loaded = json.loads([l for l in out.stdout.splitlines() if l.startswith("LOADED")][0][7:])
+    assert loaded == {"engine": False, "oracle": True}
+    rec = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][0])
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "smc-cat_b200"))
+    import bench
+    from smccat import workload
+    assert rec["config"] == bench.bench_config(workload.CONFIGS[2], 2, 1)
