@@ -465,14 +465,15 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
         fill_exp(a, i, k, spec + (size_t)k * kSpecStride, ex + (size_t)k * d.N * d.R * kStates);
     __syncthreads();
     for (int it = 0; it < gp.n_iter; ++it) {
+        // One site, uniform over all S. A site alone in its class stays put
+        // (the move never empties a class), so the site is selected with
+        // probability 1/S both ways and the selection cancels from the
+        // Metropolis-Hastings ratio: a draw from only the sites that may move
+        // would not, since moving a site changes which sites those are.
         if (threadIdx.x == 0) {
-            int s = -1;
-            for (int tries = 0; tries < 64 && s < 0; ++tries) {
-                int c = (int)((1.0 - curand_uniform_double(&rng_state)) * d.S);
-                c = c < d.S ? c : d.S - 1;
-                if (counts[assign[c]] >= 2) s = c;  // the move never empties a class
-            }
-            s_site = s;
+            int c = (int)((1.0 - curand_uniform_double(&rng_state)) * d.S);
+            c = c < d.S ? c : d.S - 1;
+            s_site = counts[assign[c]] >= 2 ? c : -1;
         }
         __syncthreads();
         const int s = s_site;

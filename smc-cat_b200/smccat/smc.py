@@ -11,7 +11,9 @@ reassignment on a random ``alg8_probability`` fraction of the particles
 Reassignment is either the reference's Gibbs move (Neal 8) or the learned
 proposal: that arm uses Gibbs for its first ``learned_warmup`` rejuvenation
 rounds, trains the MLP on the assignments they leave, then proposes with it
-(a Metropolis-Hastings move, so the target is unchanged).
+(a Metropolis-Hastings move, so the target is unchanged). The learned move
+keeps the class count fixed, so that arm still runs the Gibbs move after the
+learned one on every ``gibbs_every``-th round: the class count keeps mixing.
 
 Not in the reference: a running estimate of the log marginal likelihood,
 log Z = sum over steps of the change of logsumexp(raw weights) -- the standard
@@ -32,8 +34,8 @@ def _lse(x: np.ndarray) -> float:
 
 def run(eng, *, cat: bool, iterations: int = 20, threshold: float = 0.6,
         alg8_probability: float = 0.1, reassign: str = "gibbs", learned_warmup: int = 2,
-        learned_updates: int | None = None, seed: int = 0, max_steps: int = 100000,
-        sync=None) -> dict:
+        learned_updates: int | None = None, gibbs_every: int = 4, seed: int = 0,
+        max_steps: int = 100000, sync=None) -> dict:
     """Run the loop on all of ``eng``'s particles (loaded and refreshed).
     ``sync`` (optional) is called before reading the wall clock."""
     n = eng.P
@@ -72,7 +74,7 @@ def run(eng, *, cat: bool, iterations: int = 20, threshold: float = 0.6,
                     if use_learned:
                         eng.learned_move(updates=learned_updates or eng.S // 2, temperature=temp,
                                          seed=int(rng.integers(1 << 62)), mask=mask)
-                    else:
+                    if not use_learned or (rounds - learned_warmup) % gibbs_every == gibbs_every - 1:
                         eng.gibbs(temperature=temp, seed=int(rng.integers(1 << 62)), mask=mask)
             raw = np.full(n, -np.log(n))
             resamples += 1
