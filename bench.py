@@ -66,8 +66,9 @@ def parse():
                     help="also time the same particles with site-pattern compression")
     ap.add_argument("--mixed", type=int, default=1,
                     help="also time the FP32 (mixed-precision) path on the same particles")
-    ap.add_argument("--extra-configs", default="",
-                    help="comma-separated CAT configs (e.g. 3,4) to time in particle waves")
+    ap.add_argument("--extra-configs", default="4",
+                    help="comma-separated CAT configs (e.g. 3,4) to time in particle waves, at "
+                         "their full particle counts ('' to skip)")
     ap.add_argument("--extra-particles", type=int, default=0,
                     help="particles for --extra-configs (default: the configuration's)")
     ap.add_argument("--sampler-config", type=int, default=0,
@@ -80,7 +81,7 @@ def parse():
                          "CAT workload: plain FP64 + Gibbs against FP32 + learned proposal, "
                          "this many replicate seeds each")
     ap.add_argument("--smc-particles", type=int, default=64)
-    ap.add_argument("--gibbs-particles", type=int, default=32,
+    ap.add_argument("--gibbs-particles", type=int, default=0,
                     help="particles of a CAT --extra-configs run timed through one Gibbs pass "
                          "and one learned-proposal pass (0 to skip)")
     return ap.parse_args()
@@ -413,11 +414,21 @@ def measure_config_waves(cid, steps, local, rank, particles=0, oracle_sample=2, 
         one_pass()
         prof = eng.profile()
         eng.set_profiling(False)
-        res[name] = {"value": n * cfg.S * cfg.R / (ms * 1e-3), "unit": UNIT, "ms_per_pass": ms,
+        units = n * cfg.S * cfg.R
+        b_unit, _, b_min = algorithmic_cost(cfg.T, cfg.R, w=esz)
+        prune_s = prof["ms"]["prune"] * 1e-3
+        peak = measured_peaks()[0]
+        res[name] = {"value": units / (ms * 1e-3), "unit": UNIT, "ms_per_pass": ms,
                      "particles_per_wave": W, "waves": (n + W - 1) // W,
                      "device_gb": eng.device_bytes / 1e9,
                      "kernel_ms_per_pass": {k: round(v, 3) for k, v in prof["ms"].items()},
-                     "prune_variant": eng.kernel_variants()[1]}
+                     "prune_variant": eng.kernel_variants()[1],
+                     "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak,
+                                  "achieved": b_unit * units / prune_s / 1e9,
+                                  "frac": b_unit * units / prune_s / 1e9 / peak,
+                                  "min_bytes_frac": b_min * units / prune_s / 1e9 / peak,
+                                  "what": "pruning kernels' summed CUDA-event time over the waves "
+                                          "of one pass, algorithmic bytes (T-1)(60w+8) per unit"}}
         eng.close()
         if cfg.cat and name == "fp64" and gibbs_particles > 0:
             res["reassignment"] = measure_reassignment(codes, st, cfg, min(gibbs_particles, n),
