@@ -349,6 +349,29 @@ int smccat_propose(smccat_ctx* ctx, int32_t p, int32_t family, uint64_t seed, in
 int smccat_rejuvenate(smccat_ctx* ctx, int32_t first, int32_t count, int32_t iterations,
                       double temperature, uint64_t seed, smccat_move_stats* stats);
 
+/* Mcmc::operator()(particle, iterations, tempering) (Mcmc.cpp:25-73) for every
+ * particle of [first, first+count) with everything on the device. Each
+ * particle's sequence of moves -- per iteration one draw from the registry of
+ * main.cpp:55-106 (tree 3 x floor(T/4), stationary 1 x 2K, shape 1 x 2 when
+ * R > 1, invariant 1 x 2 with +I, rate matrix 1 x 5 without LG), repeated its
+ * count of times -- is drawn on the host from `seed`; then all particles
+ * advance in lockstep through as many steps as the longest sequence (a
+ * particle whose sequence has ended idles). Every step's proposals
+ * (Particle::treeMove, invarMove, shapeMove, stationaryMove, rateMatrixMove:
+ * Particle.cpp:677-783, with the same rules as smccat_propose), spectral
+ * decompositions, transition matrices, pruning, reduction and
+ * Metropolis-Hastings decisions on temperature * lnL + lnPrior + log Hastings
+ * run as device kernels with fixed launch shapes; with use_graph != 0 the
+ * whole sweep is captured as one CUDA graph and launched once. Draws come from
+ * a Philox stream per particle. Afterwards the host state holds every
+ * particle's final tree, branch lengths, exchangeabilities, logits, pinv and
+ * shape. Needs refreshed, committed particles (+I models: pinv > 0). stats
+ * (may be NULL) gets the per-kind counts and, as lockstep_steps, the number
+ * of steps. */
+int smccat_mcmc_sweep(smccat_ctx* ctx, int32_t first, int32_t count, int32_t iterations,
+                      double temperature, uint64_t seed, int32_t use_graph,
+                      smccat_move_stats* stats);
+
 typedef struct smccat_gibbs_stats {
     int64_t particles;       /* particles reassigned                         */
     int64_t classes_before;  /* summed class counts before                   */

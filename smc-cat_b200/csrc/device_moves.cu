@@ -27,6 +27,20 @@
 // trees (children and post-order regenerated from the parent tables), branch
 // lengths and committed workspaces back.
 //
+// smccat_mcmc_sweep runs the reference's whole Mcmc::operator() (Mcmc.cpp:25-73)
+// this way: each particle's sequence of moves -- a draw from the registry of
+// main.cpp:55-106 per iteration, repeated its count of times -- is drawn on
+// the host first, and every step of the sweep then runs that step's move for
+// each particle: the tree mixture above, or a parameter move
+// (Particle.cpp:706-783): invarMove (beta proposal on pinv; only the root
+// reduction reruns), shapeMove (rates re-discretised on the device, every
+// matrix and partial rebuilt), stationaryMove (one logit of one class shifted,
+// that class re-decomposed, every matrix and partial rebuilt) or
+// rateMatrixMove (one exchangeability, or all of them through the Cholesky
+// factor; every class re-decomposed, everything rebuilt). dm_spec_kernel
+// re-decomposes the classes a step touches; the MH kernel restores the
+// parameters (and the spectral workspaces) of rejected proposals.
+//
 // Partials invalidated by a topology move: the moved node and its ancestors,
 // and for SPR also the old parent's ancestors. (The reference's SPRMove marks
 // only the new path, Tree.cpp:803-807, leaving the old parent's partials stale
@@ -37,12 +51,15 @@
 
 #include <algorithm>
 #include <cstring>
+#include <random>
 #include <string>
 #include <vector>
 
 #include "engine_internal.h"
+#include "gamma_math.cuh"
 #include "kernels.h"
 #include "smccat.h"
+#include "spectral.cuh"
 
 namespace smccat {
 namespace {
@@ -52,7 +69,11 @@ constexpr int kDmWarps = 4;     // particles per proposal / MH block (one warp e
 constexpr int kUndo = 8;  // table edits of one move (SPR: 6, NNI: 4)
 
 // Move kinds, numbered like SMCCAT_MOVE_*.
-constexpr int kAnni = 0, kNni = 1, kSpr = 2, kBranch = 3, kSubtree = 4;
+constexpr int kAnni = 0, kNni = 1, kSpr = 2, kBranch = 3, kSubtree = 4, kInvar = 5, kShape = 6,
+              kStationary = 7, kRateSingle = 8, kRateFull = 9;
+constexpr int kKinds = 10;
+// Registry families, numbered like SMCCAT_FAMILY_*; -1 in a schedule = idle.
+constexpr int kFamTree = 0, kFamStationary = 1, kFamShape = 2, kFamInvar = 3, kFamRate = 4;
 
 struct DmArgs {
     Dims d;
@@ -84,8 +105,25 @@ struct DmArgs {
     curandStatePhilox4_32_10_t* rng;  // [count]
     double* lnl;         // engine arrays, [max_particles]
     double* lnl_old;
-    unsigned long long* stats;  // proposed / accepted per move kind (10)
+    unsigned long long* stats;  // proposed / accepted per move kind (2 x kKinds)
     double scale_delta, subtree_delta, anni_eps, temp;
+    // Whole-registry sweeps (sched != null); tree-only sweeps leave these null.
+    const int8_t* sched;    // [count][nsched] family of each step, -1 = idle
+    int nsched, step;
+    PartHdr* hdr0w;         // hdr0, writable: accepted pinv / rates are committed here
+    double* base;           // [count][kBase] exchangeabilities
+    double* logits;         // [count][Kmax][kStates]
+    double* shape;          // [count]
+    double* shape_new;      // [count] this step's proposal
+    double* undo_base;      // [count][kBase] exchangeabilities before a rate-matrix proposal
+    double* undo_logit;     // [count] the shifted logit's previous value
+    int32_t* undo_k;        // [count] class and state of the shifted logit (k * kStates + i)
+    uint8_t* sws;           // engine's spectral workspace array [max_particles][Kmax]
+    const double* spec;     // engine's spectral records
+    uint8_t* spec_flip;     // [count][Kmax] classes this step re-decomposes
+    const double* chol;     // [kBase][kBase] lower-triangular proposal factor
+    double shape_delta, stationary_delta, rate_delta, invar_alpha;
+    int lg, R;
 };
 
 __global__ void dm_init_kernel(curandStatePhilox4_32_10_t* rng, int count, int first, unsigned long long seed) {
@@ -121,9 +159,44 @@ __device__ double anni_weight(const DmArgs& a, uint64_t c0, uint64_t c1) {
     return v + (pr >= 0.0 ? 1.0 - pr : 1.0);
 }
 
-// Shared-memory bytes one particle's proposal needs (per warp).
+// Shared-memory bytes one particle's proposal needs (per warp): the tree
+// tables, and the normal draws of a rate-matrix proposal.
 __host__ __device__ inline size_t dm_warp_bytes(int N) {
-    return ((size_t)N * (8 + 16 + 8 + 4 * 6 + 3) + 15) & ~size_t(15);
+    return ((size_t)N * (8 + 16 + 8 + 4 * 6 + 3) + 8 * kBase + 15) & ~size_t(15);
+}
+
+__device__ __forceinline__ double dm_unif(curandStatePhilox4_32_10_t* rs) {
+    return 1.0 - curand_uniform_double(rs);  // [0, 1)
+}
+
+// Gamma(a, 1) variate: Marsaglia and Tsang's squeeze method (a >= 1; for
+// a < 1 the Gamma(a + 1) draw times U^(1/a)). The rejection loop is bounded;
+// its acceptance rate is above 95%.
+__device__ double dm_gamma(curandStatePhilox4_32_10_t* rs, double a) {
+    double boost = 1.0;
+    if (a < 1.0) {
+        boost = pow(dm_unif(rs) + 1e-300, 1.0 / a);
+        a += 1.0;
+    }
+    const double dd = a - 1.0 / 3.0, cc = 1.0 / sqrt(9.0 * dd);
+    for (int it = 0; it < 1000; ++it) {
+        const double x = curand_normal_double(rs);
+        double v = 1.0 + cc * x;
+        if (v <= 0.0) continue;
+        v = v * v * v;
+        const double u = dm_unif(rs);
+        if (u < 1.0 - 0.0331 * x * x * x * x) return dd * v * boost;
+        if (log(u + 1e-300) < 0.5 * x * x + dd * (1.0 - v + log(v))) return dd * v * boost;
+    }
+    return dd * boost;
+}
+
+__device__ __forceinline__ double dm_beta_lpdf(double x, double a, double b) {
+    return lgamma(a + b) - lgamma(a) - lgamma(b) + (a - 1.0) * log(x) + (b - 1.0) * log1p(-x);
+}
+
+__device__ __forceinline__ double dm_gamma_lpdf(double x, double shape, double scale) {
+    return (shape - 1.0) * log(x) - x / scale - lgamma(shape) - shape * log(scale);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -142,6 +215,24 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
     if (i >= a.count) return;  // whole warps leave together
     const Dims& d = a.d;
     const int N = d.N, T = d.T, NI = d.NI;
+    const int family = a.sched ? a.sched[(size_t)i * a.nsched + a.step] : kFamTree;
+    if (a.spec_flip)
+        for (int k = lane; k < d.Kmax; k += 32) a.spec_flip[(size_t)i * d.Kmax + k] = 0;
+    if (family < 0) {  // this particle's sweep is over: nothing to evaluate
+        PmJob* mj = a.mjobs + (size_t)i * d.Kmax * a.nchunk;
+        for (int e = lane; e < d.Kmax * a.nchunk; e += 32) mj[e] = PmJob{i, 0, 0, 0};
+        if (lane == 0) {
+            PartHdr h = a.hdr0[i];
+            h.node_off = i * NI;
+            h.node_cnt = 0;
+            h.active = 0;
+            a.hdr[i] = h;
+            a.kind[i] = -1;
+            a.nlog[i] = 0;
+            a.nundo[i] = 0;
+        }
+        return;
+    }
     unsigned char* base = dm_smem + (size_t)(threadIdx.x >> 5) * dm_warp_bytes(N);
     double* br = reinterpret_cast<double*>(base);     // N
     uint64_t* cl = reinterpret_cast<uint64_t*>(br + N);  // 2N
@@ -154,6 +245,7 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
     uint8_t* dirty = reinterpret_cast<uint8_t*>(un + N); // N
     uint8_t* cc = dirty + N;                             // N
     uint8_t* cp = cc + N;                                // N
+    double* zz = reinterpret_cast<double*>(base + (((size_t)N * (8 + 16 + 8 + 4 * 6 + 3) + 7) & ~size_t(7)));  // kBase
     int32_t* gpar = a.parent + (size_t)i * N;
     int32_t* gkids = a.kids + (size_t)i * 2 * N;
     double* gbr = a.branch + (size_t)i * N;
@@ -176,8 +268,18 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
     int kind = 0;
     if (lane == 0) {
         rs = a.rng[i];
-        const double u = 1.0 - curand_uniform_double(&rs);  // Particle.cpp:680-701
-        kind = u < 0.1 ? kNni : u < 0.4 ? kAnni : u < 0.5 ? kSpr : u < 0.9 ? kBranch : kSubtree;
+        if (family == kFamTree) {
+            const double u = 1.0 - curand_uniform_double(&rs);  // Particle.cpp:680-701
+            kind = u < 0.1 ? kNni : u < 0.4 ? kAnni : u < 0.5 ? kSpr : u < 0.9 ? kBranch : kSubtree;
+        } else if (family == kFamStationary) {
+            kind = kStationary;
+        } else if (family == kFamShape) {
+            kind = kShape;
+        } else if (family == kFamInvar) {
+            kind = kInvar;
+        } else {  // Particle.cpp:706-732: the full (Cholesky) proposal a quarter of the time
+            kind = dm_unif(&rs) < 0.25 ? kRateFull : kRateSingle;
+        }
         if (kind == kAnni && a.use_splits) {  // clades bottom-up over a pre-order walk
             int top = 0, cnt = 0;
             stk[top++] = root;
@@ -208,7 +310,10 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
     }
 
     int nord = 0, nch = 0;
-    double hastings = 0.0;
+    double hastings = 0.0, dprior = 0.0;
+    double new_pinv = a.hdr0[i].pinv;
+    double new_rates[kMaxRates];
+    for (int r = 0; r < kMaxRates; ++r) new_rates[r] = a.hdr0[i].rates[r];
     if (lane == 0) {
         int32_t* lg = a.ulog + (size_t)i * 2 * kUndo;
         double* gul = a.undo_len + (size_t)i * N;
@@ -317,6 +422,76 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
             set_kid(2 * x + 1 - s1, an);
             set_par(an, x);
             mark_paths(gp, x);
+        } else if (kind >= kInvar) {
+            // Parameter moves (Particle.cpp:706-783).
+            const int K = h0.num_classes;
+            uint8_t* flip = a.spec_flip + (size_t)i * d.Kmax;
+            double* lgt = a.logits + (size_t)i * d.Kmax * kStates;
+            double* bs = a.base + (size_t)i * kBase;
+            if (kind == kInvar) {
+                // invarMove: beta proposal centred on the current pinv.
+                const double al = a.invar_alpha, cur = h0.pinv;
+                const double aa = al + 1.0, bb = al / cur - aa + 2.0;
+                const double x = dm_gamma(&rs, aa), y = dm_gamma(&rs, bb);
+                double nv = x / (x + y);
+                nv = fmin(fmax(nv, 1e-300), 1.0 - 1e-16);
+                const double b2 = al / nv - aa + 2.0;
+                hastings = dm_beta_lpdf(cur, aa, b2) - dm_beta_lpdf(nv, aa, bb);
+                new_pinv = nv;
+            } else {
+                if (kind == kShape) {
+                    // shapeMove: multiplicative proposal, rates re-discretised.
+                    const double sc = exp(a.shape_delta * (dm_unif(&rs) - 0.5));
+                    const double old = a.shape[i], nw = old * sc;
+                    a.shape_new[i] = nw;
+                    gm_discretize_gamma(nw, a.R, new_rates);
+                    hastings = log(sc);
+                    dprior = dm_gamma_lpdf(nw, 3.0, 2.0) - dm_gamma_lpdf(old, 3.0, 2.0);
+                } else if (kind == kStationary) {
+                    // stationaryMove, with the shift applied to the class's logit.
+                    const int k = min(K - 1, (int)(dm_unif(&rs) * K));
+                    const int st = min(kStates - 1, (int)(dm_unif(&rs) * kStates));
+                    const double old = lgt[(size_t)k * kStates + st];
+                    const double nw = old + curand_normal_double(&rs) * a.stationary_delta;
+                    lgt[(size_t)k * kStates + st] = nw;
+                    a.undo_k[i] = k * kStates + st;
+                    a.undo_logit[i] = old;
+                    dprior = -0.5 * (nw * nw - old * old);
+                    flip[k] = 1;
+                } else {
+                    // rateMatrixMove: one entry, or all through the Cholesky
+                    // factor (the product runs over the lanes below).
+                    double* ub = a.undo_base + (size_t)i * kBase;
+                    for (int x = 0; x < kBase; ++x) ub[x] = bs[x];
+                    if (kind == kRateFull) {
+                        for (int x = 0; x < kBase; ++x) zz[x] = curand_normal_double(&rs);
+                    } else {
+                        const int x = min(kBase - 1, (int)(kBase * dm_unif(&rs)));
+                        const double old = bs[x];
+                        const double nw = old + curand_normal_double(&rs) * a.rate_delta;
+                        bs[x] = nw;
+                        if (!a.lg) dprior = -0.5 * (nw * nw - old * old);
+                    }
+                    for (int k = 0; k < K; ++k) flip[k] = 1;
+                }
+                // Every transition matrix and partial is rebuilt: all non-root
+                // nodes' matrices, all internal nodes in a post-order
+                // (a reversed pre-order: each node after its children).
+                int top = 0, cnt = 0;
+                stk[top++] = root;
+                while (top > 0 && cnt < N) {
+                    const int n = stk[--top];
+                    un[cnt++] = n;
+                    if (n >= T && top + 2 <= N) { stk[top++] = kids[2 * n]; stk[top++] = kids[2 * n + 1]; }
+                }
+                for (int q = cnt - 1; q >= 0; --q)
+                    if (un[q] >= T && nord < N) ord[nord++] = un[q];
+                nch = 0;
+                for (int n = 0; n < N; ++n) {
+                    dirty[n] = (n != root ? 1 : 0) | (n >= T ? 2 : 0);
+                    if (n != root) un[nch++] = n;
+                }
+            }
         } else {
             // scaleBranchMove / scaleSubtreeMove (Tree.cpp:553-612): x's
             // branch, or every branch of x's subtree (walk order: pre-order
@@ -351,12 +526,33 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
             hastings = nch * log(sc);
         }
         a.nlog[i] = nlog;
-        a.nundo[i] = nch;
+        a.nundo[i] = (kind == kBranch || kind == kSubtree) ? nch : 0;
         a.kind[i] = kind;
         a.rng[i] = rs;
     }
     nord = __shfl_sync(0xffffffffu, nord, 0);
     nch = __shfl_sync(0xffffffffu, nch, 0);
+    __syncwarp();
+    if (kind == kRateFull) {
+        // base += L z over the lanes (L lower triangular), and the N(0, 1)
+        // prior change of the exchangeabilities.
+        double* bs = a.base + (size_t)i * kBase;
+        double dp = 0.0;
+        for (int x = lane; x < kBase; x += 32) {
+            double acc = 0.0;
+            for (int j = 0; j <= x; ++j) acc = fma(a.chol[(size_t)x * kBase + j], zz[j], acc);
+            const double old = bs[x], nw = old + acc;
+            bs[x] = nw;
+            dp += -0.5 * (nw * nw - old * old);
+        }
+        dp = warp_sum(dp);
+        if (lane == 0 && !a.lg) dprior = dp;
+    }
+    if (kind >= kStationary) {  // the re-decomposed classes take their other spectral workspace
+        const uint8_t* flip = a.spec_flip + (size_t)i * d.Kmax;
+        for (int k = lane; k < d.Kmax; k += 32)
+            if (flip[k]) a.sws[(size_t)(a.first + i) * d.Kmax + k] ^= 1;
+    }
     __syncwarp();
 
     // Next workspaces, the tree and the dirty flags back to global memory.
@@ -412,11 +608,23 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
         h.node_cnt = nn;
         h.root_ws = cc[root];
         h.active = 1;
+        h.pinv = new_pinv;
+        for (int r = 0; r < kMaxRates; ++r) h.rates[r] = new_rates[r];
         a.hdr[i] = h;
-        // Tree-length prior Gamma(2T-2, scale 1/10) (Particle.cpp:484-517)
-        // and the Hastings ratio.
-        a.extra[i] = (N - 2) * (log(L1) - log(L0)) - (L1 - L0) / 0.1 + hastings;
+        // Tree-length prior Gamma(2T-2, scale 1/10) (Particle.cpp:484-517),
+        // the parameter priors' change and the Hastings ratio.
+        a.extra[i] = (N - 2) * (log(L1) - log(L0)) - (L1 - L0) / 0.1 + dprior + hastings;
     }
+}
+
+// One warp per (particle, class) slot: re-decompose the classes a step's
+// proposal marked, into the spectral workspace the proposal switched them to.
+__global__ void __launch_bounds__(32) dm_spec_kernel(DmArgs a) {
+    const int i = blockIdx.x / a.d.Kmax, k = blockIdx.x - i * a.d.Kmax;
+    if (!a.spec_flip[(size_t)i * a.d.Kmax + k]) return;
+    const size_t pk = (size_t)(a.first + i) * a.d.Kmax + k;
+    double* rec = const_cast<double*>(a.spec) + (pk * 2 + a.sws[pk]) * kSpecStride;
+    spectral_decompose_warp(a.base + (size_t)i * kBase, a.logits + ((size_t)i * a.d.Kmax + k) * kStates, rec);
 }
 
 // One warp per particle: lane 0 draws the decision, the lanes commit the
@@ -427,6 +635,7 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_mh_kernel(DmArgs a) {
     if (i >= a.count) return;  // whole warps leave together
     const int N = a.d.N, p = a.first + i;
     const int kind = a.kind[i];
+    if (kind < 0) return;  // idle this step
     int ok = 0;
     if (lane == 0) {
         curandStatePhilox4_32_10_t rs = a.rng[i];
@@ -459,12 +668,30 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_mh_kernel(DmArgs a) {
             if (f & 2) kc[n] = a.cur_clws[(size_t)i * N + n];
             if (f & 1) kp[n] = a.cur_pws[(size_t)i * N + n];
         }
+        // Accepted parameters: pinv and rates become the committed header;
+        // exchangeabilities, logits and spectral workspaces already are.
+        if (lane == 0 && (kind == kInvar || kind == kShape)) {
+            a.hdr0w[i].pinv = a.hdr[i].pinv;
+            for (int r = 0; r < kMaxRates; ++r) a.hdr0w[i].rates[r] = a.hdr[i].rates[r];
+            if (kind == kShape) a.shape[i] = a.shape_new[i];
+        }
     } else {
         // The scaled nodes are distinct: their lengths restore in any order.
         double* br = a.branch + (size_t)i * N;
         const int32_t* un = a.undo_node + (size_t)i * N;
         const double* ul = a.undo_len + (size_t)i * N;
         for (int q = lane; q < a.nundo[i]; q += 32) br[un[q]] = ul[q];
+        // Rejected parameters: previous exchangeabilities or logit, and the
+        // re-decomposed classes back on their previous spectral workspace.
+        if (kind == kRateSingle || kind == kRateFull)
+            for (int x = lane; x < kBase; x += 32) a.base[(size_t)i * kBase + x] = a.undo_base[(size_t)i * kBase + x];
+        if (kind == kStationary && lane == 0)
+            a.logits[(size_t)i * a.d.Kmax * kStates + a.undo_k[i]] = a.undo_logit[i];
+        if (kind >= kStationary) {
+            const uint8_t* flip = a.spec_flip + (size_t)i * a.d.Kmax;
+            for (int k = lane; k < a.d.Kmax; k += 32)
+                if (flip[k]) a.sws[(size_t)p * a.d.Kmax + k] ^= 1;
+        }
     }
 }
 
@@ -473,15 +700,12 @@ int dm_fail(int code, const std::string& msg) {
     return code;
 }
 
-}  // namespace
-}  // namespace smccat
-
-using namespace smccat;
-
-extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, int32_t steps,
-                                 double temperature, uint64_t seed, int32_t use_graph,
-                                 int64_t* stats) {
-    if (!c) return dm_fail(SMCCAT_EINVAL, "null context");
+// A device-resident sweep of `steps` lockstep MH steps on [first, first+count).
+// sched (count x steps, row-major) gives each particle's move family per step
+// (-1 = idle); null runs the tree mixture at every step. kind_stats gets
+// proposed / accepted counts per move kind (2 x kKinds).
+int device_sweep(smccat_ctx* c, int first, int count, int steps, const std::vector<int8_t>* sched,
+                 double temperature, uint64_t seed, int use_graph, unsigned long long* kind_stats) {
     const Dims& d = dims_of(c);
     if (first < 0 || count < 1 || steps < 0) return dm_fail(SMCCAT_EINVAL, "bad range");
     for (int i = 0; i < count; ++i) {
@@ -507,8 +731,12 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
     std::vector<double> br((size_t)count * N);
     std::vector<uint8_t> clws((size_t)count * N), pws((size_t)count * N);
     std::vector<PartHdr> hdr0(count);
+    // The committed spectral workspaces: the device array holds what the last
+    // refresh shipped, which a later reject on the host path may have undone.
+    std::vector<uint8_t> sws0((size_t)count * d.Kmax);
     for (int i = 0; i < count; ++i) {
         const Mirror& m = slot_of(c, first + i).cur;
+        std::copy(m.sws.begin(), m.sws.end(), &sws0[(size_t)i * d.Kmax]);
         std::copy(m.parent.begin(), m.parent.end(), &par[(size_t)i * N]);
         std::copy(m.kids.begin(), m.kids.end(), &kids[(size_t)i * 2 * N]);
         std::copy(m.branch.begin(), m.branch.end(), &br[(size_t)i * N]);
@@ -548,7 +776,25 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
                  o_hdr0 = take((size_t)count * sizeof(PartHdr)), o_hdr = take((size_t)count * sizeof(PartHdr)),
                  o_nodes = take((size_t)count * NI * sizeof(NodeJob)), o_pj = take(cN * sizeof(PJob)),
                  o_mj = take((size_t)count * d.Kmax * nchunk * sizeof(PmJob)),
-                 o_rng = take((size_t)count * sizeof(curandStatePhilox4_32_10_t)), o_stats = take(10 * 8);
+                 o_rng = take((size_t)count * sizeof(curandStatePhilox4_32_10_t)),
+                 o_stats = take(2 * kKinds * 8);
+    // Parameter state of whole-registry sweeps.
+    const bool params = sched != nullptr;
+    const size_t cK = (size_t)count * d.Kmax;
+    size_t o_sched = 0, o_base = 0, o_logits = 0, o_shape = 0, o_shape_new = 0, o_ubase = 0,
+           o_ulogit = 0, o_uk = 0, o_flip = 0, o_chol = 0;
+    if (params) {
+        o_sched = take((size_t)count * steps);
+        o_base = take((size_t)count * kBase * 8);
+        o_logits = take(cK * kStates * 8);
+        o_shape = take((size_t)count * 8);
+        o_shape_new = take((size_t)count * 8);
+        o_ubase = take((size_t)count * kBase * 8);
+        o_ulogit = take((size_t)count * 8);
+        o_uk = take((size_t)count * 4);
+        o_flip = take(cK);
+        o_chol = take((size_t)kBase * kBase * 8);
+    }
     unsigned char* buf = moves_buffer(c, off);
     if (!buf) return dm_fail(SMCCAT_ENOMEM, "device-move buffers: out of device memory");
     a.parent = reinterpret_cast<int32_t*>(buf + o_par);
@@ -575,6 +821,42 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
     a.mjobs = reinterpret_cast<PmJob*>(buf + o_mj);
     a.rng = reinterpret_cast<curandStatePhilox4_32_10_t*>(buf + o_rng);
     a.stats = reinterpret_cast<unsigned long long*>(buf + o_stats);
+    std::vector<double> h_base, h_logits, h_shape, h_chol;
+    if (params) {
+        a.sched = reinterpret_cast<const int8_t*>(buf + o_sched);
+        a.nsched = steps;
+        a.hdr0w = reinterpret_cast<PartHdr*>(buf + o_hdr0);
+        a.base = reinterpret_cast<double*>(buf + o_base);
+        a.logits = reinterpret_cast<double*>(buf + o_logits);
+        a.shape = reinterpret_cast<double*>(buf + o_shape);
+        a.shape_new = reinterpret_cast<double*>(buf + o_shape_new);
+        a.undo_base = reinterpret_cast<double*>(buf + o_ubase);
+        a.undo_logit = reinterpret_cast<double*>(buf + o_ulogit);
+        a.undo_k = reinterpret_cast<int32_t*>(buf + o_uk);
+        a.spec_flip = buf + o_flip;
+        a.chol = reinterpret_cast<const double*>(buf + o_chol);
+        a.sws = const_cast<uint8_t*>(v.sws);
+        a.spec = v.spec;
+        a.shape_delta = tn.shape_delta;
+        a.stationary_delta = tn.stationary_delta;
+        a.rate_delta = tn.rate_matrix_delta;
+        a.invar_alpha = tn.invar_alpha;
+        a.lg = (model_flags_of(c) & SMCCAT_MODEL_LG) ? 1 : 0;
+        a.R = d.R;
+        h_base.resize((size_t)count * kBase);
+        h_logits.assign(cK * kStates, 0.0);
+        h_shape.resize(count);
+        h_chol.resize((size_t)kBase * kBase);
+        for (int i = 0; i < count; ++i) {
+            const Mirror& m = slot_of(c, first + i).cur;
+            std::copy(m.base.begin(), m.base.end(), &h_base[(size_t)i * kBase]);
+            std::copy(m.logits.begin(), m.logits.begin() + (size_t)m.K * kStates,
+                      &h_logits[(size_t)i * d.Kmax * kStates]);
+            h_shape[i] = m.shape;
+        }
+        rc = smccat_get_rate_cholesky(c, h_chol.data());
+        if (rc) return rc;
+    }
 
     cudaStream_t st = v.st;
     cudaGraph_t graph = nullptr;
@@ -597,7 +879,17 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
     DM_CK(cudaMemcpyAsync(a.clws, clws.data(), cN, cudaMemcpyHostToDevice, st));
     DM_CK(cudaMemcpyAsync(a.pws, pws.data(), cN, cudaMemcpyHostToDevice, st));
     DM_CK(cudaMemcpyAsync(buf + o_hdr0, hdr0.data(), (size_t)count * sizeof(PartHdr), cudaMemcpyHostToDevice, st));
-    DM_CK(cudaMemsetAsync(a.stats, 0, 10 * 8, st));
+    DM_CK(cudaMemsetAsync(a.stats, 0, 2 * kKinds * 8, st));
+    DM_CK(cudaMemcpyAsync(const_cast<uint8_t*>(v.sws) + (size_t)first * d.Kmax, sws0.data(), sws0.size(),
+                          cudaMemcpyHostToDevice, st));
+    if (params) {
+        DM_CK(cudaMemcpyAsync(buf + o_sched, sched->data(), (size_t)count * steps, cudaMemcpyHostToDevice, st));
+        DM_CK(cudaMemcpyAsync(a.base, h_base.data(), h_base.size() * 8, cudaMemcpyHostToDevice, st));
+        DM_CK(cudaMemcpyAsync(a.logits, h_logits.data(), h_logits.size() * 8, cudaMemcpyHostToDevice, st));
+        DM_CK(cudaMemcpyAsync(a.shape, h_shape.data(), h_shape.size() * 8, cudaMemcpyHostToDevice, st));
+        DM_CK(cudaMemcpyAsync(buf + o_chol, h_chol.data(), h_chol.size() * 8, cudaMemcpyHostToDevice, st));
+        DM_CK(cudaMemsetAsync(a.spec_flip, 0, cK, st));
+    }
     if (nsplit > 0) {
         DM_CK(cudaMemcpyAsync(buf + o_sk, skeys.data(), (size_t)nsplit * 16, cudaMemcpyHostToDevice, st));
         DM_CK(cudaMemcpyAsync(buf + o_sp, sprob.data(), (size_t)nsplit * 8, cudaMemcpyHostToDevice, st));
@@ -623,14 +915,20 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
     pa.hdr = a.hdr;
     pa.nodes = a.nodes;
     const int nmjobs = count * d.Kmax * nchunk;
-    auto step = [&]() -> cudaError_t {
-        dm_propose_kernel<<<pgrid, 32 * pwarps, psmem, st>>>(a);
+    auto step = [&](int k) -> cudaError_t {
+        DmArgs ak = a;
+        ak.step = k;
+        dm_propose_kernel<<<pgrid, 32 * pwarps, psmem, st>>>(ak);
         cudaError_t x = cudaGetLastError();
+        if (x == cudaSuccess && params) {
+            dm_spec_kernel<<<count * d.Kmax, 32, 0, st>>>(ak);
+            x = cudaGetLastError();
+        }
         if (x == cudaSuccess) x = launch_pmat(a.mjobs, nmjobs, a.pjobs, a.hdr, first, v.sws, v.spec, v.Pm, v.fp32, d, st);
         if (x == cudaSuccess) x = launch_prune(pa, v.ntiles, v.variant, st);
         if (x == cudaSuccess) x = launch_reduce(v.tile_off, pa.partial, a.hdr, first, count, v.lnl, v.status, st);
         if (x == cudaSuccess) {
-            dm_mh_kernel<<<(count + kDmWarps - 1) / kDmWarps, 32 * kDmWarps, 0, st>>>(a);
+            dm_mh_kernel<<<(count + kDmWarps - 1) / kDmWarps, 32 * kDmWarps, 0, st>>>(ak);
             x = cudaGetLastError();
         }
         return x;
@@ -639,18 +937,27 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
         if (use_graph) {
             DM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
             cudaError_t x = cudaSuccess;
-            for (int k = 0; k < steps && x == cudaSuccess; ++k) x = step();
+            for (int k = 0; k < steps && x == cudaSuccess; ++k) x = step(k);
             const cudaError_t y = cudaStreamEndCapture(st, &graph);
             DM_CK(x);
             DM_CK(y);
             DM_CK(cudaGraphInstantiate(&exec, graph, 0));
             DM_CK(cudaGraphLaunch(exec, st));
         } else {
-            for (int k = 0; k < steps; ++k) DM_CK(step());
+            for (int k = 0; k < steps; ++k) DM_CK(step(k));
         }
     }
-    unsigned long long h_stats[10];
+    unsigned long long h_stats[2 * kKinds];
     int status = 0;
+    std::vector<uint8_t> h_sws;
+    if (params) {
+        h_sws.resize(cK);
+        DM_CK(cudaMemcpyAsync(h_base.data(), a.base, h_base.size() * 8, cudaMemcpyDeviceToHost, st));
+        DM_CK(cudaMemcpyAsync(h_logits.data(), a.logits, h_logits.size() * 8, cudaMemcpyDeviceToHost, st));
+        DM_CK(cudaMemcpyAsync(h_shape.data(), a.shape, h_shape.size() * 8, cudaMemcpyDeviceToHost, st));
+        DM_CK(cudaMemcpyAsync(hdr0.data(), buf + o_hdr0, (size_t)count * sizeof(PartHdr), cudaMemcpyDeviceToHost, st));
+        DM_CK(cudaMemcpyAsync(h_sws.data(), v.sws + (size_t)first * d.Kmax, cK, cudaMemcpyDeviceToHost, st));
+    }
     DM_CK(cudaMemcpyAsync(h_stats, a.stats, sizeof(h_stats), cudaMemcpyDeviceToHost, st));
     DM_CK(cudaMemcpyAsync(&status, v.status, sizeof(int), cudaMemcpyDeviceToHost, st));
     DM_CK(cudaMemcpyAsync(br.data(), a.branch, cN * 8, cudaMemcpyDeviceToHost, st));
@@ -679,10 +986,94 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
             std::copy(&br[(size_t)i * N], &br[(size_t)i * N] + N, m->branch.begin());
             std::copy(&clws[(size_t)i * N], &clws[(size_t)i * N] + N, m->clws.begin());
             std::copy(&pws[(size_t)i * N], &pws[(size_t)i * N] + N, m->pws.begin());
+            if (params) {
+                std::copy(&h_base[(size_t)i * kBase], &h_base[(size_t)i * kBase] + kBase, m->base.begin());
+                std::copy(&h_logits[(size_t)i * d.Kmax * kStates],
+                          &h_logits[(size_t)i * d.Kmax * kStates] + (size_t)m->K * kStates, m->logits.begin());
+                m->shape = h_shape[i];
+                m->pinv = hdr0[i].pinv;
+                for (int r = 0; r < kMaxRates; ++r) m->rates[r] = hdr0[i].rates[r];
+                std::copy(&h_sws[(size_t)i * d.Kmax], &h_sws[(size_t)i * d.Kmax] + d.Kmax, m->sws.begin());
+            }
         }
     }
-    if (stats)
-        for (int k = 0; k < 10; ++k) stats[k] = (int64_t)h_stats[k];
+    if (kind_stats)
+        for (int k = 0; k < 2 * kKinds; ++k) kind_stats[k] = h_stats[k];
     return finish(SMCCAT_OK, "");
 #undef DM_CK
+}
+
+}  // namespace
+}  // namespace smccat
+
+using namespace smccat;
+
+extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, int32_t steps,
+                                 double temperature, uint64_t seed, int32_t use_graph,
+                                 int64_t* stats) {
+    if (!c) return dm_fail(SMCCAT_EINVAL, "null context");
+    unsigned long long ks[2 * kKinds];
+    const int rc = device_sweep(c, first, count, steps, nullptr, temperature, seed, use_graph, ks);
+    if (rc) return rc;
+    if (stats)
+        for (int k = 0; k < 10; ++k) stats[k] = (int64_t)ks[k];
+    return SMCCAT_OK;
+}
+
+extern "C" int smccat_mcmc_sweep(smccat_ctx* c, int32_t first, int32_t count, int32_t iterations,
+                                 double temperature, uint64_t seed, int32_t use_graph,
+                                 smccat_move_stats* stats) {
+    if (!c) return dm_fail(SMCCAT_EINVAL, "null context");
+    if (first < 0 || count < 1 || iterations < 0) return dm_fail(SMCCAT_EINVAL, "bad range");
+    const Dims& d = dims_of(c);
+    const int flags = model_flags_of(c);
+    for (int i = 0; i < count; ++i) {
+        const Slot& s = slot_of(c, first + i);
+        if (!s.loaded) return dm_fail(SMCCAT_ESTATE, "particle has no state loaded");
+        if ((flags & SMCCAT_MODEL_INVAR) && !(s.cur.pinv > 0.0))
+            return dm_fail(SMCCAT_EINVAL, "invariant-site move needs pinv > 0");
+    }
+    // The registry of main.cpp:55-106 (weight, family), Mcmc::initMoveProbs
+    // (Mcmc.cpp:15-23), and each particle's step sequence: per iteration one
+    // draw from the registry, repeated its count of times (Mcmc.cpp:40-56).
+    struct Entry { double w; int family; };
+    std::vector<Entry> reg{{3.0, kFamTree}, {1.0, kFamStationary}};
+    if (d.R > 1) reg.push_back({1.0, kFamShape});
+    if (flags & SMCCAT_MODEL_INVAR) reg.push_back({1.0, kFamInvar});
+    if (!(flags & SMCCAT_MODEL_LG)) reg.push_back({1.0, kFamRate});
+    double wt = 0.0;
+    for (auto& e : reg) wt += e.w;
+    std::vector<double> cum;
+    double acc = 0.0;
+    for (auto& e : reg) { acc += e.w; cum.push_back(acc / wt); }
+    std::vector<std::vector<int8_t>> seq(count);
+    size_t steps = 0;
+    for (int i = 0; i < count; ++i) {
+        std::mt19937_64 g(seed * 0x9E3779B97F4A7C15ull + (uint64_t)(first + i) + 1);
+        const int K = slot_of(c, first + i).cur.K;
+        for (int it = 0; it < iterations; ++it) {
+            const double u = std::generate_canonical<double, 53>(g);
+            int fam = reg.back().family;
+            for (size_t j = 0; j < cum.size(); ++j)
+                if (u < cum[j]) { fam = reg[j].family; break; }
+            const int rep = fam == kFamTree ? (int)(d.T * 0.25) : fam == kFamStationary ? 2 * K
+                          : fam == kFamRate ? 5 : 2;
+            seq[i].insert(seq[i].end(), rep, (int8_t)fam);
+        }
+        steps = std::max(steps, seq[i].size());
+    }
+    std::vector<int8_t> sched((size_t)count * steps, (int8_t)-1);
+    for (int i = 0; i < count; ++i) std::copy(seq[i].begin(), seq[i].end(), &sched[(size_t)i * steps]);
+    unsigned long long ks[2 * kKinds];
+    const int rc = device_sweep(c, first, count, (int)steps, &sched, temperature, seed, use_graph, ks);
+    if (rc) return rc;
+    if (stats) {
+        *stats = smccat_move_stats{};
+        for (int k = 0; k < kKinds; ++k) {
+            stats->proposed[k] = ks[2 * k];
+            stats->accepted[k] = ks[2 * k + 1];
+        }
+        stats->lockstep_steps = steps;
+    }
+    return SMCCAT_OK;
 }

@@ -141,6 +141,8 @@ def lib():
         "smccat_propose": ([vp, _i32, _i32, ctypes.c_uint64, _ip, _dp], ctypes.c_int),
         "smccat_rejuvenate": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64,
                                ctypes.POINTER(MoveStats)], ctypes.c_int),
+        "smccat_mcmc_sweep": ([vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_uint64, _i32,
+                               ctypes.POINTER(MoveStats)], ctypes.c_int),
         "smccat_smc_step": ([vp, _i32, _i32, _dp, ctypes.c_double, ctypes.c_double, _dp, _dp,
                              _dp], ctypes.c_int),
         "smccat_gibbs": ([vp, _i32, _i32, _up, ctypes.c_double, ctypes.c_uint64,
@@ -415,6 +417,18 @@ class Engine:
         st = MoveStats()
         _check(lib().smccat_rejuvenate(self._h, int(first), int(count), int(iterations),
                                        float(temperature), int(seed), ctypes.byref(st)))
+        return {"proposed": list(st.proposed), "accepted": list(st.accepted),
+                "lockstep_steps": int(st.lockstep_steps)}
+
+    def mcmc_sweep(self, iterations, temperature, seed, use_graph=True, first=0,
+                   count=None) -> dict:
+        """Mcmc::operator() on every particle with everything on the device
+        (smccat_mcmc_sweep); the whole sweep is one CUDA graph by default."""
+        count = self.P - first if count is None else count
+        st = MoveStats()
+        _check(lib().smccat_mcmc_sweep(self._h, int(first), int(count), int(iterations),
+                                       float(temperature), int(seed), 1 if use_graph else 0,
+                                       ctypes.byref(st)))
         return {"proposed": list(st.proposed), "accepted": list(st.accepted),
                 "lockstep_steps": int(st.lockstep_steps)}
 
