@@ -71,11 +71,11 @@ def parse():
                          "their full particle counts ('' to skip)")
     ap.add_argument("--extra-particles", type=int, default=0,
                     help="particles for --extra-configs (default: the configuration's)")
-    ap.add_argument("--sampler-config", type=int, default=0,
-                    help="CAT config (e.g. 4) on which to compare sampler sweeps/s: plain FP64 + "
-                         "Gibbs against FP32 + learned proposal (0 to skip)")
-    ap.add_argument("--sampler-particles", type=int, default=32)
-    ap.add_argument("--sampler-sweeps", type=int, default=1)
+    ap.add_argument("--sampler-config", type=int, default=4,
+                    help="CAT config on which to compare sampler sweeps/s and ESS/s: plain FP64 + "
+                         "Gibbs against FP32 + device graph sweep + learned proposal (0 to skip)")
+    ap.add_argument("--sampler-particles", type=int, default=48)
+    ap.add_argument("--sampler-sweeps", type=int, default=4)
     ap.add_argument("--smc", type=int, default=0,
                     help="run whole SMC analyses (temperature 0 -> 1) on a 16-taxon x 500-site "
                          "CAT workload: plain FP64 + Gibbs against FP32 + learned proposal, "
@@ -253,67 +253,143 @@ def measure_reassignment(codes, st, cfg, n, local, torch):
                         "acceptance": ls["accepted"] / max(ls["proposed"], 1)}}
 
 
-def measure_sampler(cid, n, sweeps, local, torch):
-    """Sampler sweeps/s on a CAT configuration. One sweep = Mcmc::operator()
-    with the configuration's iterations on every particle (lockstep) + one CAT
-    reassignment pass of floor(S/2) site updates per particle. Plain arm: FP64
-    partials, Gibbs (Neal 8). Chosen arm: FP32 partials, the learned proposal,
-    its MLP trained (untimed) on the assignments one Gibbs warm-up pass leaves.
-    The chosen arm's final states are re-evaluated in FP64 for its |dlogL|.
-    Wall clock around device-synchronised calls."""
+def multichain_ess(x):
+    """Effective sample size of m chains of n draws, x [m][n] (Gelman et al.,
+    Bayesian Data Analysis 3rd ed., 11.5): the pooled variance estimate
+    var+ = (n-1)/n W + B/n, autocorrelations rho_t = 1 - V_t / (2 var+) from
+    the variogram V_t, summed over lags while adjacent pairs stay positive."""
+    x = np.asarray(x, dtype=np.float64)
+    m, n = x.shape
+    if n < 2:
+        return float("nan")
+    W = x.var(axis=1, ddof=1).mean()
+    B_over_n = x.mean(axis=1).var(ddof=1) if m > 1 else 0.0
+    var_plus = (n - 1) / n * W + B_over_n
+    if not var_plus > 0:
+        return float("nan")
+    rho = []
+    for t in range(1, n):
+        V = np.mean((x[:, t:] - x[:, :-t]) ** 2)
+        rho.append(1.0 - V / (2.0 * var_plus))
+    s = 0.0
+    for t in range(0, len(rho), 2):
+        pair = rho[t] + (rho[t + 1] if t + 1 < len(rho) else 0.0)
+        if pair < 0:
+            break
+        s += pair
+    return float(m * n / (1.0 + 2.0 * s))
+
+
+def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=4):
+    """The north-star sampler comparison on a CAT configuration.
+
+    One sweep = Mcmc::operator() with the configuration's iterations on every
+    particle + one CAT reassignment pass of floor(S/2) site updates per
+    particle, at temperature 1.
+      plain arm:  FP64 partials; Mcmc::operator() on the host-driven lockstep
+                  path (smccat_rejuvenate); Neal-8 Gibbs reassignment.
+      chosen arm: FP32 partials; Mcmc::operator() entirely on the device as one
+                  CUDA graph (smccat_mcmc_sweep); the learned-proposal
+                  reassignment, with the Gibbs move on every `gibbs_every`-th
+                  sweep so the class count keeps mixing. Its MLP is trained
+                  (untimed) on the assignments a Gibbs warm-up pass leaves.
+    Both arms start from the same particles and run one untimed warm-up sweep,
+    then `sweeps` timed ones (wall clock around device-synchronised calls).
+    After every timed sweep the log-likelihood, tree length and class count of
+    every particle are recorded; their multi-chain ESS over the particles
+    divided by the arm's seconds is its ESS/s. The chosen arm's final states
+    are re-evaluated at FP64 for its |dlogL|."""
     import smccat
     from smccat import workload
     cfg = workload.CONFIGS[cid]
     codes, _ = workload.simulate_alignment(cfg, np.random.default_rng(cfg.seed))
     st = workload.make_particles(cfg, n, np.random.default_rng(cfg.seed * 7 + 1))
-    kmax = st["logits"].shape[1] + 32
+    kmax = st["logits"].shape[1] + 96  # room for the classes Gibbs opens
     logits = np.zeros((n, kmax, 20))
     logits[:, :st["logits"].shape[1]] = st["logits"]
-    res = {"workload": cfg.name, "particles": n, "sweeps": sweeps,
+    res = {"workload": cfg.name, "particles": n, "timed_sweeps": sweeps,
            "sweep": f"Mcmc::operator() x {cfg.iterations} iterations + {cfg.S // 2} site updates "
-                    "per particle, temperature 1"}
-    engines = {}
-    for arm, prec in (("plain_fp64_gibbs", smccat.PREC_FP64), ("fp32_learned", smccat.PREC_FP32)):
+                    "per particle, temperature 1",
+           "particles_note": f"{n} particles resident per arm (FP64 partials of a "
+                             f"{cfg.T}x{cfg.S} particle with {kmax} class slots take ~2 GB)"}
+    finals = {}
+    for arm, prec in (("plain_fp64_gibbs", smccat.PREC_FP64), ("fp32_graph_learned", smccat.PREC_FP32)):
         eng = smccat.Engine(codes, cfg.R, n, max_classes=kmax, lg=cfg.lg, invar=cfg.invar,
                             cat=cfg.cat, device=local, precision=prec)
         eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"], logits,
                           st["assign"], st["pinv"], st["shape"])
         eng.refresh(full=True)
+        eng.compute_split_posteriors()
+        chosen = arm != "plain_fp64_gibbs"
         info = {}
-        if arm == "fp32_learned":
+
+        def sweep(k, timed):
+            out = {}
+            if chosen:
+                r = eng.mcmc_sweep(iterations=cfg.iterations, temperature=1.0, seed=100 + k)
+                g = eng.learned_move(updates=cfg.S // 2, temperature=1.0, seed=200 + k)
+                out["acc"] = g["accepted"] / max(g["proposed"], 1)
+                if timed and k % gibbs_every == gibbs_every - 1:
+                    eng.gibbs(temperature=1.0, seed=300 + k)
+                    out["gibbs"] = True
+            else:
+                r = eng.rejuvenate(iterations=cfg.iterations, temperature=1.0, seed=100 + k)
+                eng.gibbs(temperature=1.0, seed=200 + k)
+            out["steps"] = r["lockstep_steps"]
+            out["mh"] = (sum(r["accepted"]), sum(r["proposed"]))
+            return out
+
+        if chosen:
             eng.gibbs(temperature=1.0, seed=1)
             info["train_loss"] = eng.learned_train(epochs=1, batch_sites=512, lr=1e-3, seed=2,
                                                    first=0, count=min(n, 8))
+        sweep(-1, False)  # warm-up (also graph capture of the first kind)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        steps, acc = 0, []
+        traces = {"lnl": [], "tree_length": [], "classes": []}
+        secs, steps, acc, mh_a, mh_p, n_gibbs = 0.0, 0, [], 0, 0, 0
         for k in range(sweeps):
-            r = eng.rejuvenate(iterations=cfg.iterations, temperature=1.0, seed=100 + k)
-            steps += r["lockstep_steps"]
-            if arm == "plain_fp64_gibbs":
-                eng.gibbs(temperature=1.0, seed=200 + k)
-            else:
-                g = eng.learned_move(updates=cfg.S // 2, temperature=1.0, seed=200 + k)
-                acc.append(g["accepted"] / max(g["proposed"], 1))
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        info.update({"sweeps_per_s": sweeps / (t1 - t0), "seconds_per_sweep": (t1 - t0) / sweeps,
-                     "lockstep_steps_per_sweep": steps / sweeps})
+            t0 = time.perf_counter()
+            o = sweep(k, True)
+            torch.cuda.synchronize()
+            secs += time.perf_counter() - t0
+            steps += o["steps"]
+            mh_a += o["mh"][0]
+            mh_p += o["mh"][1]
+            n_gibbs += 1 if (not chosen or o.get("gibbs")) else 0
+            if "acc" in o:
+                acc.append(o["acc"])
+            print(f"sampler {arm} sweep {k}: {time.perf_counter() - t0:.2f} s, {o['steps']} steps",
+                  file=sys.stderr, flush=True)
+            g = eng.get_particles()
+            traces["lnl"].append(eng.lnl())
+            traces["tree_length"].append(g["branch"].sum(axis=1))
+            traces["classes"].append(g["num_classes"].astype(np.float64))
+        ess = {k: multichain_ess(np.stack(v, axis=1)) for k, v in traces.items()}
+        info.update({"sweeps_per_s": sweeps / secs, "seconds_per_sweep": secs / sweeps,
+                     "lockstep_steps_per_sweep": steps / sweeps,
+                     "mcmc_acceptance": mh_a / max(mh_p, 1), "gibbs_passes": n_gibbs,
+                     "ess": ess, "ess_per_s": {k: v / secs for k, v in ess.items()},
+                     "mean_lnl_last": float(np.mean(traces["lnl"][-1])),
+                     "mean_classes_last": float(np.mean(traces["classes"][-1]))})
         if acc:
             info["learned_acceptance"] = float(np.mean(acc))
         res[arm] = info
-        engines[arm] = eng
+        finals[arm] = (eng.get_particles(), eng.lnl())
+        eng.close()
     # FP64 re-evaluation of the chosen arm's final states.
-    e32, e64 = engines["fp32_learned"], engines["plain_fp64_gibbs"]
-    l32 = e32.lnl()
-    g = e32.get_particles()
+    g, l32 = finals["fp32_graph_learned"]
+    e64 = smccat.Engine(codes, cfg.R, n, max_classes=kmax, lg=cfg.lg, invar=cfg.invar, cat=cfg.cat,
+                        device=local)
     e64.set_particles(0, g["parent"], g["branch"], g["base"], g["num_classes"], g["logits"],
                       g["assign"], g["pinv"], g["shape"])
     e64.refresh(full=True)
-    res["fp32_learned"]["max_abs_dlogl_vs_fp64"] = float(np.max(np.abs(l32 - e64.lnl())))
-    for e in engines.values():
-        e.close()
-    res["speedup_sweeps_per_s"] = res["fp32_learned"]["sweeps_per_s"] / res["plain_fp64_gibbs"]["sweeps_per_s"]
+    res["fp32_graph_learned"]["max_abs_dlogl_vs_fp64"] = float(np.max(np.abs(l32 - e64.lnl())))
+    e64.close()
+    p, c = res["plain_fp64_gibbs"], res["fp32_graph_learned"]
+    res["speedup_sweeps_per_s"] = c["sweeps_per_s"] / p["sweeps_per_s"]
+    res["ess_per_s_ratio"] = {k: (c["ess_per_s"][k] / p["ess_per_s"][k])
+                              if p["ess_per_s"][k] and np.isfinite(p["ess_per_s"][k]) else None
+                              for k in p["ess_per_s"]}
     return res
 
 
