@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
         __syncwarp();
     }
 
-    int nord = 0, nch = 0;
+    int nord = 0, nch = 0, local_k = -1;
     double hastings = 0.0, dprior = 0.0;
     double new_pinv = a.hdr0[i].pinv;
     double new_rates[kMaxRates];
@@ -458,6 +458,7 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
                     a.undo_logit[i] = old;
                     dprior = -0.5 * (nw * nw - old * old);
                     flip[k] = 1;
+                    local_k = k;
                 } else {
                     // rateMatrixMove: one entry, or all through the Cholesky
                     // factor (the product runs over the lanes below).
@@ -476,7 +477,10 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
                 }
                 // Every transition matrix and partial is rebuilt: all non-root
                 // nodes' matrices, all internal nodes in a post-order
-                // (a reversed pre-order: each node after its children).
+                // (a reversed pre-order: each node after its children). A
+                // stationary move rebuilds its class alone, class-locally: the
+                // node workspaces stay (no dirty flags), that class's byte of
+                // the spectral-workspace array flips its own workspaces.
                 int top = 0, cnt = 0;
                 stk[top++] = root;
                 while (top > 0 && cnt < N) {
@@ -488,7 +492,7 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
                     if (un[q] >= T && nord < N) ord[nord++] = un[q];
                 nch = 0;
                 for (int n = 0; n < N; ++n) {
-                    dirty[n] = (n != root ? 1 : 0) | (n >= T ? 2 : 0);
+                    dirty[n] = kind == kStationary ? 0 : (n != root ? 1 : 0) | (n >= T ? 2 : 0);
                     if (n != root) un[nch++] = n;
                 }
             }
@@ -532,6 +536,7 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
     }
     nord = __shfl_sync(0xffffffffu, nord, 0);
     nch = __shfl_sync(0xffffffffu, nch, 0);
+    local_k = __shfl_sync(0xffffffffu, local_k, 0);
     __syncwarp();
     if (kind == kRateFull) {
         // base += L z over the lanes (L lower triangular), and the N(0, 1)
@@ -550,8 +555,9 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
     }
     if (kind >= kStationary) {  // the re-decomposed classes take their other spectral workspace
         const uint8_t* flip = a.spec_flip + (size_t)i * d.Kmax;
+        const uint8_t fl = kind == kStationary ? (kSwsSpec | kSwsCl | kSwsP) : kSwsSpec;
         for (int k = lane; k < d.Kmax; k += 32)
-            if (flip[k]) a.sws[(size_t)(a.first + i) * d.Kmax + k] ^= 1;
+            if (flip[k]) a.sws[(size_t)(a.first + i) * d.Kmax + k] ^= fl;
     }
     __syncwarp();
 
@@ -599,7 +605,8 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
     PmJob* mj = a.mjobs + (size_t)i * d.Kmax * a.nchunk;
     for (int e = lane; e < d.Kmax * a.nchunk; e += 32) {
         const int k = e / a.nchunk, c = e - k * a.nchunk;
-        const int nj_k = k < h0.num_classes ? max(0, min(kPmChunk, nch - kPmChunk * c)) : 0;
+        const bool cls_on = local_k >= 0 ? k == local_k : k < h0.num_classes;
+        const int nj_k = cls_on ? max(0, min(kPmChunk, nch - kPmChunk * c)) : 0;
         mj[e] = PmJob{i, k, i * N + kPmChunk * c, nj_k};
     }
     if (lane == 0) {
@@ -608,6 +615,7 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
         h.node_cnt = nn;
         h.root_ws = cc[root];
         h.active = 1;
+        h.cls_only = local_k;
         h.pinv = new_pinv;
         for (int r = 0; r < kMaxRates; ++r) h.rates[r] = new_rates[r];
         a.hdr[i] = h;
@@ -623,7 +631,7 @@ __global__ void __launch_bounds__(32) dm_spec_kernel(DmArgs a) {
     const int i = blockIdx.x / a.d.Kmax, k = blockIdx.x - i * a.d.Kmax;
     if (!a.spec_flip[(size_t)i * a.d.Kmax + k]) return;
     const size_t pk = (size_t)(a.first + i) * a.d.Kmax + k;
-    double* rec = const_cast<double*>(a.spec) + (pk * 2 + a.sws[pk]) * kSpecStride;
+    double* rec = const_cast<double*>(a.spec) + (pk * 2 + (a.sws[pk] & kSwsSpec)) * kSpecStride;
     spectral_decompose_warp(a.base + (size_t)i * kBase, a.logits + ((size_t)i * a.d.Kmax + k) * kStates, rec);
 }
 
@@ -688,9 +696,10 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_mh_kernel(DmArgs a) {
         if (kind == kStationary && lane == 0)
             a.logits[(size_t)i * a.d.Kmax * kStates + a.undo_k[i]] = a.undo_logit[i];
         if (kind >= kStationary) {
+            const uint8_t fl = kind == kStationary ? (kSwsSpec | kSwsCl | kSwsP) : kSwsSpec;
             const uint8_t* flip = a.spec_flip + (size_t)i * a.d.Kmax;
             for (int k = lane; k < a.d.Kmax; k += 32)
-                if (flip[k]) a.sws[(size_t)p * a.d.Kmax + k] ^= 1;
+                if (flip[k]) a.sws[(size_t)p * a.d.Kmax + k] ^= fl;
         }
     }
 }
@@ -746,6 +755,7 @@ int device_sweep(smccat_ctx* c, int first, int count, int steps, const std::vect
         std::memset(&h, 0, sizeof(h));
         h.root = m.root;
         h.num_classes = m.K;
+        h.cls_only = -1;
         h.pinv = m.pinv;
         for (int r = 0; r < kMaxRates; ++r) h.rates[r] = m.rates[r];
     }

@@ -514,6 +514,11 @@ int smccat_set_particles(smccat_ctx* c, int32_t first, int32_t count, const int3
         m.shape = shape[i];
         discretize_gamma(m.shape, d.R, m.rates);
         s.assign.assign(assign + (size_t)i * S, assign + (size_t)(i + 1) * S);
+        // A loaded state is rebuilt and committed whole: the classes' workspace
+        // flips restart at zero (class numbers may mean other classes now).
+        for (Mirror* mm : {&s.cur, &s.old})
+            for (auto& b : mm->sws) b &= kSwsSpec;
+        s.local_class = -1;
         s.loaded = true;
         s.full = true;
         s.commit_on_refresh = true;
@@ -592,6 +597,15 @@ int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
 
 }  // extern "C"
 
+// A pending class-local edit with nothing else dirty: the refresh can rebuild
+// that class alone.
+static bool local_plan(const Slot& s) {
+    if (s.local_class < 0 || s.full) return false;
+    for (size_t n = 0; n < s.dirty_cl.size(); ++n)
+        if (s.dirty_cl[n] || s.dirty_p[n]) return false;
+    return true;
+}
+
 int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, const uint8_t* active) {
     int rc = check_range(c, first, count);
     if (rc) return rc;
@@ -635,6 +649,17 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
                 x.nn = (int)m.post.size();
                 x.np = N - 1;
                 x.ns = m.K;
+            } else if (local_plan(s)) {
+                x.nn = (int)m.post.size();
+                x.np = N - 1;
+                x.ns = 1;
+                x.nm = (x.np + kPmChunk - 1) / kPmChunk;  // class local_class only
+                cn[i + 1] = x;
+                continue;
+            } else if (s.local_class >= 0) {  // a class edit combined with others: everything
+                x.nn = (int)m.post.size();
+                x.np = N - 1;
+                for (int k = 0; k < m.K; ++k) x.ns += s.dirty_spec[k];
             } else {
                 for (int n : m.post) x.nn += s.dirty_cl[n];
                 for (int n = 0; n < N; ++n) x.np += (s.dirty_p[n] && n != m.root);
@@ -681,16 +706,67 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
             continue;
         }
         const bool full = (mode == SMCCAT_REFRESH_FULL) || s.full;
+        if (!full && local_plan(s)) {
+            // Class-local refresh (a stationary edit of one class): that class
+            // is re-decomposed, its matrices of every node and its sites'
+            // partials of every internal node rebuilt into its other
+            // workspaces (all three workspace bits of its byte flip); node
+            // workspace indices stay, and the other classes' tiles only rerun
+            // the root reduction.
+            const int k = s.local_class;
+            m.sws[k] = s.old.sws[k] ^ (kSwsSpec | kSwsCl | kSwsP);
+            SpecJob& j = sjobs[js++];
+            j.p = p; j.k = k; j.sws = m.sws[k] & kSwsSpec; j.pad = 0;
+            std::memcpy(j.base, m.base.data(), sizeof(j.base));
+            std::memcpy(j.logits, &m.logits[(size_t)k * kStates], sizeof(j.logits));
+            const int pj0 = jp;
+            for (int n = 0; n < N; ++n)
+                if (n != m.root) pjobs[jp++] = PJob{p, n, m.pws[n], 0, m.branch[n]};
+            for (int q = pj0; q < jp; q += kPmChunk)
+                mjobs[jm++] = PmJob{i, k, q, std::min(kPmChunk, jp - q)};
+            PartHdr& h = hdr[i];
+            h.node_off = jn;
+            for (int n : m.post) {
+                const int c1 = m.kids[2 * n], c2 = m.kids[2 * n + 1];
+                int ws = m.clws[n];
+                if (c1 >= d.T) ws |= m.clws[c1] << 1;
+                if (c2 >= d.T) ws |= m.clws[c2] << 2;
+                ws |= m.pws[c1] << 3;
+                ws |= m.pws[c2] << 4;
+                nodes[jn++] = NodeJob{n, c1, c2, ws};
+            }
+            h.node_cnt = jn - h.node_off;
+            h.root = m.root;
+            h.root_ws = m.clws[m.root];
+            h.active = 1;
+            h.num_classes = m.K;
+            h.cls_only = k;
+            h.pad1 = 0;
+            h.pinv = m.pinv;
+            for (int r = 0; r < kMaxRates; ++r) h.rates[r] = m.rates[r];
+            std::fill(s.dirty_spec.begin(), s.dirty_spec.end(), 0);
+            s.local_class = -1;
+            s.full = false;
+            s.refreshed = true;
+            std::copy(m.sws.begin(), m.sws.end(), c->h_sws + (size_t)p * Kmax);
+            continue;
+        }
+        if (s.local_class >= 0) {  // combined with other edits: rebuild everything
+            std::fill(s.dirty_p.begin(), s.dirty_p.end(), 1);
+            for (int n : m.post) s.dirty_cl[n] = 1;
+            s.local_class = -1;
+        }
         if (full) {
             std::fill(s.dirty_spec.begin(), s.dirty_spec.begin() + m.K, 1);
             std::fill(s.dirty_p.begin(), s.dirty_p.end(), 1);
             for (int n : m.post) s.dirty_cl[n] = 1;
+            s.local_class = -1;
         }
         for (int k = 0; k < m.K; ++k) {
             if (!s.dirty_spec[k]) continue;
-            m.sws[k] = 1 - s.old.sws[k];
+            m.sws[k] = s.old.sws[k] ^ kSwsSpec;
             SpecJob& j = sjobs[js++];
-            j.p = p; j.k = k; j.sws = m.sws[k]; j.pad = 0;
+            j.p = p; j.k = k; j.sws = m.sws[k] & kSwsSpec; j.pad = 0;
             std::memcpy(j.base, m.base.data(), sizeof(j.base));
             std::memcpy(j.logits, &m.logits[(size_t)k * kStates], sizeof(j.logits));
         }
@@ -722,7 +798,8 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
         h.root_ws = m.clws[m.root];
         h.active = 1;
         h.num_classes = m.K;
-        h.pad0 = h.pad1 = 0;
+        h.cls_only = -1;
+        h.pad1 = 0;
         h.pinv = m.pinv;
         for (int r = 0; r < kMaxRates; ++r) h.rates[r] = m.rates[r];
         std::fill(s.dirty_spec.begin(), s.dirty_spec.end(), 0);
@@ -913,7 +990,8 @@ int smccat_get_transition_matrix(smccat_ctx* c, int32_t p, int32_t k, int32_t no
         return fail(SMCCAT_EINVAL, "bad class / node / rate index");
     if (s.pending && !s.refreshed) return fail(SMCCAT_ESTATE, "particle has unrefreshed edits");
     unsigned char blk[kPBlock * 8];
-    const size_t off = ((((size_t)p * d.Kmax + k) * d.N + node) * 2 + s.cur.pws[node]) *
+    const int pws = s.cur.pws[node] ^ ((s.cur.sws[k] & kSwsP) ? 1 : 0);
+    const size_t off = ((((size_t)p * d.Kmax + k) * d.N + node) * 2 + pws) *
                            (size_t)d.R * kPBlock + (size_t)r * kPBlock;
     CK(cudaSetDevice(c->cfg.device));
     CK(d2h(c, blk, c->d_Pm + off * c->esz, (size_t)kPBlock * c->esz));
@@ -1020,9 +1098,20 @@ int smccat_set_class_logits(smccat_ctx* c, int32_t p, int32_t k, const double* l
     Slot& s = c->slots[p];
     if (!logits || k < 0 || k >= s.cur.K) return fail(SMCCAT_EINVAL, "bad class index");
     std::copy(logits, logits + kStates, s.cur.logits.begin() + (size_t)k * kStates);
+    // Alone, the edit is class-local: only class k's matrices and sites are
+    // rebuilt, into that class's other workspaces. With other edits pending
+    // (or a second class edited) everything is rebuilt.
+    bool others = s.full || s.local_class >= 0;
+    for (int i = 0; i < c->d.N && !others; ++i) others = s.dirty_cl[i] || s.dirty_p[i];
+    for (int j = 0; j < s.cur.K && !others; ++j) others = s.dirty_spec[j] && j != k;
     s.dirty_spec[k] = 1;
-    std::fill(s.dirty_p.begin(), s.dirty_p.end(), 1);
-    for (int n : s.cur.post) s.dirty_cl[n] = 1;
+    if (!others && !s.pending) {
+        s.local_class = k;
+    } else {
+        s.local_class = -1;
+        std::fill(s.dirty_p.begin(), s.dirty_p.end(), 1);
+        for (int n : s.cur.post) s.dirty_cl[n] = 1;
+    }
     s.pending = true;
     return SMCCAT_OK;
 }
@@ -1051,6 +1140,7 @@ int smccat_accept(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* ma
         Slot& s = c->slots[first + i];
         if (mask[i]) s.old = s.cur;
         else s.cur = s.old;
+        s.local_class = -1;
         std::fill(s.dirty_spec.begin(), s.dirty_spec.end(), 0);
         std::fill(s.dirty_p.begin(), s.dirty_p.end(), 0);
         std::fill(s.dirty_cl.begin(), s.dirty_cl.end(), 0);

@@ -57,6 +57,8 @@ struct Slot {
     bool commit_on_refresh = false;
     bool pending = false;       // edits since the last commit
     bool refreshed = false;     // refreshed since the last commit
+    int local_class = -1;       // >= 0: the only pending edit is that class's logits,
+                                // refreshed class-locally (its own workspace flips)
 };
 
 // Refresh particles [first, first+count); `active` (count bytes, may be

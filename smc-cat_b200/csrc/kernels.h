@@ -15,6 +15,22 @@ struct Dims {
     int T, S, Spad, R, N, NI, Kmax;
 };
 
+// The byte of the spectral-workspace array of (particle p, class k): bit 0 is
+// the class's spectral workspace; bits 1 and 2 flip the partial and
+// transition-matrix workspaces of that class's sites and matrices. A
+// class-local move (one class's stationary frequencies) rebuilds that class
+// alone into the other workspaces by flipping those bits, leaving the node
+// workspace indices, and so every other class, untouched.
+constexpr uint8_t kSwsSpec = 1, kSwsCl = 2, kSwsP = 4;
+#ifdef __CUDACC__
+// NodeJob.ws bits to flip for a tile or matrix of class k: the three partial
+// workspaces (node, child 1, child 2) with bit 1, the two matrix ones with bit 2.
+__device__ __forceinline__ int class_ws_flip(const uint8_t* sws, int p, int Kmax, int k) {
+    const int b = sws[(size_t)p * Kmax + k];
+    return ((b & kSwsCl) ? 7 : 0) | ((b & kSwsP) ? 24 : 0);
+}
+#endif
+
 struct PruneArgs {
     Dims d;
     int first;        // first particle of the refresh range (hdr index base)

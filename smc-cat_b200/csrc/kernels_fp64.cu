@@ -161,7 +161,7 @@ __device__ __forceinline__ void matvec(const T* __restrict__ P, const T (*x)[kSt
 __global__ void __launch_bounds__(32) spec_kernel(const SpecJob* __restrict__ jobs,
                                                   double* __restrict__ spec, Dims d) {
     const SpecJob* job = jobs + blockIdx.x;
-    double* rec = spec + (((size_t)job->p * d.Kmax + job->k) * 2 + job->sws) * kSpecStride;
+    double* rec = spec + (((size_t)job->p * d.Kmax + job->k) * 2 + (job->sws & kSwsSpec)) * kSpecStride;
     spectral_decompose_warp(job->base, job->logits, rec);
 }
 
@@ -198,8 +198,8 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
     __shared__ double ex[kPmChunk][kMaxRates][kStates];
     __shared__ size_t obase[kPmChunk];
     const int tid = threadIdx.x;
-    const double* rec =
-        spec + (((size_t)p * d.Kmax + mj.k) * 2 + sws[(size_t)p * d.Kmax + mj.k]) * kSpecStride;
+    const uint8_t sb = sws[(size_t)p * d.Kmax + mj.k];
+    const double* rec = spec + (((size_t)p * d.Kmax + mj.k) * 2 + (sb & kSwsSpec)) * kSpecStride;
     for (int idx = tid; idx < kStates * kStates; idx += kPmThreads) {
         const int a = idx / kStates, b = idx % kStates;
         Lt[b][pm_ilv(a, 5)] = rec[kSpecL + idx];
@@ -214,7 +214,8 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
     }
     if (tid < mj.nj) {
         const PJob pj = jobs[mj.j0 + tid];
-        obase[tid] = ((((size_t)p * d.Kmax + mj.k) * d.N + pj.node) * 2 + pj.pws) * (size_t)d.R * kPBlock;
+        const int pws = pj.pws ^ ((sb & kSwsP) ? 1 : 0);  // the class's matrix-workspace flip
+        obase[tid] = ((((size_t)p * d.Kmax + mj.k) * d.N + pj.node) * 2 + pws) * (size_t)d.R * kPBlock;
     }
     __syncthreads();
     // Every exponential of the chunk in one phase, then no barrier per node.
@@ -334,12 +335,16 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     __syncthreads();
     if (!h->active) return true;  // uniform across the CTA (after the barriers exist)
 
-    const int cnt = h->node_cnt;
+    // A class-local refresh of another class leaves this tile's partials as
+    // they are: only its root reduction reruns.
+    const int cnt = (h->cls_only >= 0 && h->cls_only != tl.k) ? 0 : h->node_cnt;
+    const int wfl = class_ws_flip(a.sws, p, d.Kmax, tl.k);
     const NodeJob* nodes = a.nodes + h->node_off;
     uint32_t pend = 0;  // lane 0: bit b set while a copy into buffer b is not yet waited on
     if (cnt > 0 && lane == 0) {
         fence_proxy_async();  // a previous tile's root rows were written here
-        const NodeJob nj = nodes[0];
+        NodeJob nj = nodes[0];
+        nj.ws ^= wfl;
         mbar_expect_tx(&bars[r][0], 2 * kPBytes);
         tma_load_1d(buf, pblock(nj.c1, (nj.ws >> 3) & 1), kPBytes, &bars[r][0]);
         tma_load_1d(buf + kPBlock, pblock(nj.c2, (nj.ws >> 4) & 1), kPBytes, &bars[r][0]);
@@ -354,10 +359,12 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     bool ok = true;
     for (int q = 0; q < cnt; ++q) {
         const int b = q & 1;
-        const NodeJob nj = nodes[q];
+        NodeJob nj = nodes[q];
+        nj.ws ^= wfl;
         if (ok && q + 1 < cnt && lane == 0) {
             // Buffer b^1 was last read at node q-1 (the warp synchronised after it).
-            const NodeJob nx = nodes[q + 1];
+            NodeJob nx = nodes[q + 1];
+            nx.ws ^= wfl;
             fence_proxy_async();
             mbar_expect_tx(&bars[r][b ^ 1], 2 * kPBytes);
             tma_load_1d(buf + (b ^ 1) * 2 * kPBlock, pblock(nx.c1, (nx.ws >> 3) & 1), kPBytes,
@@ -496,8 +503,9 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     __syncwarp();  // the warp's buffers are free from here on (red(r) reuses them)
     // Root reduction for this tile.
     if (cnt == 0 && valid) {
-        const T* xp = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride;
-        const double* lp = LSCp + (size_t)(h->root - d.T) * 2 * lws_stride + h->root_ws * lws_stride;
+        const int rws = h->root_ws ^ (wfl & 1);
+        const T* xp = CLp + (size_t)(h->root - d.T) * node_stride + rws * ws_stride;
+        const double* lp = LSCp + (size_t)(h->root - d.T) * 2 * lws_stride + rws * lws_stride;
 #pragma unroll
         for (int w = 0; w < W; ++w) {
 #pragma unroll
@@ -506,7 +514,7 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
         }
     }
     const double* rec =
-        a.spec + (((size_t)p * d.Kmax + tl.k) * 2 + a.sws[(size_t)p * d.Kmax + tl.k]) * kSpecStride;
+        a.spec + (((size_t)p * d.Kmax + tl.k) * 2 + (a.sws[(size_t)p * d.Kmax + tl.k] & kSwsSpec)) * kSpecStride;
     const double* pi = rec + kSpecPi;
     if (valid) {
 #pragma unroll

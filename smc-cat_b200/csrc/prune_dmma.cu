@@ -135,11 +135,13 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_dmma_kernel(const PruneArg
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    const int cnt = h->node_cnt;
+    const int cnt = (h->cls_only >= 0 && h->cls_only != tl.k) ? 0 : h->node_cnt;
+    const int wfl = class_ws_flip(a.sws, p, d.Kmax, tl.k);
     const NodeJob* nodes = a.nodes + h->node_off;
     uint32_t pend = 0;  // lane 0: bit b set while a copy into buffer b is not yet waited on
     if (cnt > 0 && lane == 0) {
-        const NodeJob nj = nodes[0];
+        NodeJob nj = nodes[0];
+        nj.ws ^= wfl;
         bar_expect(&bars[r][0], 2 * kPBytesD);
         bulk_load(buf, pblock(nj.c1, (nj.ws >> 3) & 1), kPBytesD, &bars[r][0]);
         bulk_load(buf + kPBlock, pblock(nj.c2, (nj.ws >> 4) & 1), kPBytesD, &bars[r][0]);
@@ -155,9 +157,11 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_dmma_kernel(const PruneArg
     uint32_t phase = 0;
     for (int q = 0; q < cnt; ++q) {
         const int b = q & 1;
-        const NodeJob nj = nodes[q];
+        NodeJob nj = nodes[q];
+        nj.ws ^= wfl;
         if (ok && q + 1 < cnt && lane == 0) {  // no new copies once a wait has given up
-            const NodeJob nx = nodes[q + 1];
+            NodeJob nx = nodes[q + 1];
+            nx.ws ^= wfl;
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             bar_expect(&bars[r][b ^ 1], 2 * kPBytesD);
             bulk_load(buf + (b ^ 1) * 2 * kPBlock, pblock(nx.c1, (nx.ws >> 3) & 1), kPBytesD,
@@ -312,7 +316,7 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_dmma_kernel(const PruneArg
     }
     // ---- root reduction
     if (cnt == 0) {
-        const double* rp = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride + colbase;
+        const double* rp = CLp + (size_t)(h->root - d.T) * node_stride + (h->root_ws ^ (wfl & 1)) * ws_stride + colbase;
 #pragma unroll
         for (int mt = 0; mt < 4; ++mt) {
 #pragma unroll
@@ -322,12 +326,12 @@ __global__ void __launch_bounds__(32 * R, MINB) prune_dmma_kernel(const PruneArg
                     const int i = 8 * nt + 2 * t + hh;
                     y[mt][nt][hh] = (sv[mt] && i < kStates) ? rp[(size_t)i * j_stride + 8 * mt + g] : 0.0;
                 }
-            lsc[mt] = sv[mt] ? LSCp[(size_t)(h->root - d.T) * 2 * lws_stride + h->root_ws * lws_stride +
+            lsc[mt] = sv[mt] ? LSCp[(size_t)(h->root - d.T) * 2 * lws_stride + (h->root_ws ^ (wfl & 1)) * lws_stride +
                                     colbase + 8 * mt + g] : 0.0;
         }
     }
     const double* rec =
-        a.spec + (((size_t)p * d.Kmax + tl.k) * 2 + a.sws[(size_t)p * d.Kmax + tl.k]) * kSpecStride;
+        a.spec + (((size_t)p * d.Kmax + tl.k) * 2 + (a.sws[(size_t)p * d.Kmax + tl.k] & kSwsSpec)) * kSpecStride;
     const double* pi = rec + kSpecPi;
 #pragma unroll
     for (int mt = 0; mt < 4; ++mt) {

@@ -183,12 +183,14 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
     const uint32_t tm = tmem_slot;
     const uint32_t tlane = tm + ((uint32_t)(warp * 32) << 16);  // this warp's lane quarter
 
-    const int cnt = h->node_cnt;
+    const int cnt = (h->cls_only >= 0 && h->cls_only != tl.k) ? 0 : h->node_cnt;
+    const int wfl = class_ws_flip(a.sws, p, d.Kmax, tl.k);
     const NodeJob* nodes = a.nodes + h->node_off;
     const int nsteps = cnt * R;  // (rate, node) pairs, rate-major
     auto issue = [&](int f) {    // thread 0: stage the P blocks of step f
         const int r = f / cnt, q = f - r * cnt;
-        const NodeJob nj = nodes[q];
+        NodeJob nj = nodes[q];
+        nj.ws ^= wfl;
         float* dst = pbuf + (size_t)(f & 1) * 2 * kPBlock;
         tc_bar_expect(&bars[f & 1], 2 * kPBytesF);
         tc_bulk(dst, pblock(nj.c1, (nj.ws >> 3) & 1, r), kPBytesF, &bars[f & 1]);
@@ -210,7 +212,7 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
     float y[kStates];
     double lsc = 0.0;
     int prev = -1;
-    const double* rec = a.spec + (((size_t)p * d.Kmax + tl.k) * 2 + a.sws[(size_t)p * d.Kmax + tl.k]) * kSpecStride;
+    const double* rec = a.spec + (((size_t)p * d.Kmax + tl.k) * 2 + (a.sws[(size_t)p * d.Kmax + tl.k] & kSwsSpec)) * kSpecStride;
     const double* pi = rec + kSpecPi;
 
     for (int r = 0; r < R; ++r) {
@@ -218,7 +220,8 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
         for (int q = 0; q < cnt; ++q) {
             const int f = r * cnt + q;
             const int b = f & 1;
-            const NodeJob nj = nodes[q];
+            NodeJob nj = nodes[q];
+            nj.ws ^= wfl;
             if (tid == 0 && ok && f + 1 < nsteps) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 issue(f + 1);  // buffer b ^ 1 was last read at step f - 1 (synchronised since)
@@ -374,10 +377,11 @@ __global__ void __launch_bounds__(kTcSites, 4) prune_tc_kernel(const PruneArgs a
         // Root value of rate r for this thread's site.
         if (cnt == 0) {
             const size_t col = (size_t)r * d.Spad + slot;
-            const float* xp = CLp + (size_t)(h->root - d.T) * node_stride + h->root_ws * ws_stride;
+            const int rws = h->root_ws ^ (wfl & 1);
+            const float* xp = CLp + (size_t)(h->root - d.T) * node_stride + rws * ws_stride;
 #pragma unroll
             for (int j = 0; j < kStates; ++j) y[j] = xp[col + j * j_stride];
-            lsc = LSCp[(size_t)(h->root - d.T) * 2 * lws_stride + h->root_ws * lws_stride + col];
+            lsc = LSCp[(size_t)(h->root - d.T) * 2 * lws_stride + rws * lws_stride + col];
         }
         double s = 0.0;
 #pragma unroll

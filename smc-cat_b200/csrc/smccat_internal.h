@@ -16,6 +16,8 @@
 //   spec    [P][Kmax][2][SPEC_STRIDE]   eigenvalues, left/right factors, pi
 // Every workspace index (CL, P, spectral) is chosen by the host mirror and
 // shipped in the per-refresh plan, so accept/reject never touches the device.
+// The partial and matrix workspace of (node, class) is the node's index XOR
+// the class's flip bit (bits 1 and 2 of its spectral-workspace byte).
 #pragma once
 #include <stdint.h>
 
@@ -47,7 +49,9 @@ struct PartHdr {
     int32_t root_ws;    // CL workspace of the root after this refresh
     int32_t active;     // 0: particle not part of this refresh
     int32_t num_classes;
-    int32_t pad0, pad1;
+    int32_t cls_only;   // >= 0: a class-local refresh of that class; the other
+                        // classes' tiles only re-run the root reduction
+    int32_t pad1;
     double pinv;
     double rates[kMaxRates];
 };
