@@ -280,7 +280,7 @@ def multichain_ess(x):
     return float(m * n / (1.0 + 2.0 * s))
 
 
-def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=4):
+def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=10, chosen_sweeps=10):
     """The north-star sampler comparison on a CAT configuration.
 
     One sweep = Mcmc::operator() with the configuration's iterations on every
@@ -291,10 +291,12 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=4):
       chosen arm: FP32 partials; Mcmc::operator() entirely on the device as one
                   CUDA graph (smccat_mcmc_sweep); the learned-proposal
                   reassignment, with the Gibbs move on every `gibbs_every`-th
-                  sweep so the class count keeps mixing. Its MLP is trained
+                  sweep so the class count keeps mixing (every 10th: the
+                  reference's rate, alg8Probability = 0.1, main.cpp:303). Its MLP is trained
                   (untimed) on the assignments a Gibbs warm-up pass leaves.
     Both arms start from the same particles and run one untimed warm-up sweep,
-    then `sweeps` timed ones (wall clock around device-synchronised calls).
+    then timed ones (wall clock around device-synchronised calls): `sweeps`
+    for the plain arm, `chosen_sweeps` (a whole Gibbs period) for the chosen one.
     After every timed sweep the log-likelihood, tree length and class count of
     every particle are recorded; their multi-chain ESS over the particles
     divided by the arm's seconds is its ESS/s. The chosen arm's final states
@@ -307,7 +309,9 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=4):
     kmax = st["logits"].shape[1] + 96  # room for the classes Gibbs opens
     logits = np.zeros((n, kmax, 20))
     logits[:, :st["logits"].shape[1]] = st["logits"]
-    res = {"workload": cfg.name, "particles": n, "timed_sweeps": sweeps,
+    res = {"workload": cfg.name, "particles": n,
+           "timed_sweeps": {"plain_fp64_gibbs": sweeps, "fp32_graph_learned": chosen_sweeps},
+           "chosen_gibbs_every": gibbs_every,
            "sweep": f"Mcmc::operator() x {cfg.iterations} iterations + {cfg.S // 2} site updates "
                     "per particle, temperature 1",
            "particles_note": f"{n} particles resident per arm (FP64 partials of a "
@@ -347,7 +351,8 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=4):
         torch.cuda.synchronize()
         traces = {"lnl": [], "tree_length": [], "classes": []}
         secs, steps, acc, mh_a, mh_p, n_gibbs = 0.0, 0, [], 0, 0, 0
-        for k in range(sweeps):
+        nsw = chosen_sweeps if chosen else sweeps
+        for k in range(nsw):
             t0 = time.perf_counter()
             o = sweep(k, True)
             torch.cuda.synchronize()
@@ -365,8 +370,8 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=4):
             traces["tree_length"].append(g["branch"].sum(axis=1))
             traces["classes"].append(g["num_classes"].astype(np.float64))
         ess = {k: multichain_ess(np.stack(v, axis=1)) for k, v in traces.items()}
-        info.update({"sweeps_per_s": sweeps / secs, "seconds_per_sweep": secs / sweeps,
-                     "lockstep_steps_per_sweep": steps / sweeps,
+        info.update({"sweeps_per_s": nsw / secs, "seconds_per_sweep": secs / nsw,
+                     "lockstep_steps_per_sweep": steps / nsw,
                      "mcmc_acceptance": mh_a / max(mh_p, 1), "gibbs_passes": n_gibbs,
                      "ess": ess, "ess_per_s": {k: v / secs for k, v in ess.items()},
                      "mean_lnl_last": float(np.mean(traces["lnl"][-1])),
