@@ -215,12 +215,16 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
     for (int k = threadIdx.x; k < Kcap + kAux; k += blockDim.x) counts[k] = 0;
     __syncthreads();
     for (int x = threadIdx.x; x < d.S; x += blockDim.x) atomicAdd(&counts[assign[x]], 1);
+    // Classes [0, K0) read their site log-likelihoods from the table; the
+    // others (none without a table) are pruned per site below.
+    const int K0 = a.table ? gp.K : 0;
+    const double* tab = a.table ? a.table + (size_t)i * a.Kt * d.S : nullptr;
     if (warp < kAux)  // one shared workspace per decomposing warp
-        for (int k = warp; k < gp.K; k += kAux)
+        for (int k = K0 + warp; k < gp.K; k += kAux)
             spectral_decompose_warp_ws(base, logits + (size_t)k * kStates,
                                        spec + (size_t)k * kSpecStride, work[warp]);
     __syncthreads();
-    for (int k = 0; k < gp.K; ++k)
+    for (int k = K0; k < gp.K; ++k)
         fill_exp(a, i, k, spec + (size_t)k * kSpecStride, ex + (size_t)k * d.N * d.R * kStates);
     __syncthreads();
 
@@ -258,7 +262,7 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
         __syncthreads();
         // 3. site log-likelihood per (class, rate) (Particle.cpp:857-930): one
         // warp per class, all its rates together
-        for (int k = warp; k < kcur + kAux; k += kGibbsWarps) {
+        for (int k = K0 + warp; k < kcur + kAux; k += kGibbsWarps) {
             if (k >= kcur || counts[k] > 0) {
                 for (int r0 = 0; r0 < d.R; r0 += kRateBlock)
                     site_class_lnl<kRateBlock>(a, i, r0, spec + (size_t)k * kSpecStride,
@@ -274,7 +278,9 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
             double wmax = -INFINITY;
             for (int k = 0; k < kcur + kAux; ++k) {
                 double w = -INFINITY;
-                if (k >= kcur || counts[k] > 0) {
+                if (k < K0 && counts[k] > 0) {
+                    w = tab[(size_t)k * d.S + s] * a.temp + log((double)counts[k]);
+                } else if (k >= kcur || counts[k] > 0) {
                     double mx = -INFINITY;
                     for (int r = 0; r < d.R; ++r) mx = fmax(mx, sh[k * d.R + r]);
                     double lse = mx;

@@ -36,6 +36,11 @@ struct GibbsArgs {
     const double* isinv;
     const int32_t* invchar;
     int* status;            // bit 4: class capacity exhausted
+    // Optional [count][Kt][S]: every site's log-likelihood (+I mixed) under each
+    // class the particle enters with, evaluated beforehand by the pruning
+    // kernels; those classes then need no single-site pruning per iteration.
+    const double* table;
+    int Kt;
     // scratch, set by launch_gibbs
     double* spec;
     double* expt;

@@ -54,6 +54,14 @@ struct PruneArgs {
     double* partial;
     int* status;      // bit 1: NaN likelihood, bit 2: a bounded wait gave up
     uint32_t wait_limit;  // polls per bounded wait (kDrainPolls unless a test lowers it)
+    // Evaluation mode (eval_k >= 0, SIMT kernels only): every tile is pruned
+    // under class eval_k instead of its own class and each site's
+    // log-likelihood goes to eval_out[j][Kmax][S], j = eval_map[p - first]
+    // (particles with j < 0, or fewer classes, are skipped); the tile
+    // partials are not written. The plan's partial workspaces are scratch.
+    int eval_k = -1;
+    const int32_t* eval_map = nullptr;
+    double* eval_out = nullptr;
 };
 
 cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d, cudaStream_t st);
@@ -70,6 +78,8 @@ int prune_variant_tile_sites(int R, bool fp32, int variant);
 // another: the fastest measured on B200 for the bench workloads.
 int prune_default_variant(int R, bool fp32);
 cudaError_t launch_prune(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
+// Whether a variant is one of the SIMT kernels (the ones with evaluation mode).
+bool prune_variant_has_eval(int R, bool fp32, int variant);
 int prune_dmma_variants(int R);
 cudaError_t launch_prune_dmma(const PruneArgs& a, int ntiles, int variant, cudaStream_t st);
 // FP32 tensor-core (tcgen05, 3xTF32) kernels: 128-slot tiles.

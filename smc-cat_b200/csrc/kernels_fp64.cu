@@ -320,8 +320,12 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     const size_t lws_stride = j_stride;
     T* CLp = static_cast<T*>(a.CL) + (size_t)p * d.NI * node_stride;
     double* LSCp = a.LSC + (size_t)p * d.NI * 2 * lws_stride;
+    // The class whose matrices and frequencies the tile runs: its own, or the
+    // class under evaluation.
+    const int ek = a.eval_k;
+    const int kc = ek >= 0 ? ek : tl.k;
     const T* Pcls = static_cast<const T*>(a.Pm) +
-                    ((size_t)p * d.Kmax + tl.k) * d.N * 2 * (size_t)R * kPBlock + (size_t)r * kPBlock;
+                    ((size_t)p * d.Kmax + kc) * d.N * 2 * (size_t)R * kPBlock + (size_t)r * kPBlock;
     auto pblock = [&](int child, int pws) {
         return Pcls + ((size_t)child * 2 + pws) * (size_t)R * kPBlock;
     };
@@ -334,11 +338,16 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     }
     __syncthreads();
     if (!h->active) return true;  // uniform across the CTA (after the barriers exist)
+    const int ej = ek >= 0 ? a.eval_map[p - a.first] : 0;
+    if (ek >= 0 && (ej < 0 || ek >= h->num_classes)) return true;  // uniform as well
 
     // A class-local refresh of another class leaves this tile's partials as
-    // they are: only its root reduction reruns.
-    const int cnt = (h->cls_only >= 0 && h->cls_only != tl.k) ? 0 : h->node_cnt;
-    const int wfl = class_ws_flip(a.sws, p, d.Kmax, tl.k);
+    // they are: only its root reduction reruns. In evaluation mode the plan
+    // names the free partial workspaces (the tile's own class flips them like
+    // the committed ones) and the evaluated class's matrices.
+    const int cnt = (ek < 0 && h->cls_only >= 0 && h->cls_only != tl.k) ? 0 : h->node_cnt;
+    const int wfl = ek >= 0 ? (class_ws_flip(a.sws, p, d.Kmax, tl.k) & 7) | (class_ws_flip(a.sws, p, d.Kmax, ek) & 24)
+                            : class_ws_flip(a.sws, p, d.Kmax, tl.k);
     const NodeJob* nodes = a.nodes + h->node_off;
     uint32_t pend = 0;  // lane 0: bit b set while a copy into buffer b is not yet waited on
     if (cnt > 0 && lane == 0) {
@@ -514,7 +523,7 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
         }
     }
     const double* rec =
-        a.spec + (((size_t)p * d.Kmax + tl.k) * 2 + (a.sws[(size_t)p * d.Kmax + tl.k] & kSwsSpec)) * kSpecStride;
+        a.spec + (((size_t)p * d.Kmax + kc) * 2 + (a.sws[(size_t)p * d.Kmax + kc] & kSwsSpec)) * kSpecStride;
     const double* pi = rec + kSpecPi;
     if (valid) {
 #pragma unroll
@@ -555,12 +564,16 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
                 u = lse + log1p(-pinv);
             }
             if (bad) u = NAN;
+            if (ek >= 0) {
+                a.eval_out[((size_t)ej * d.Kmax + ek) * d.S + site[w]] = u;
+                continue;
+            }
             a.site_lnl[(size_t)p * d.S + site[w]] = u;
             // A compressed slot stands for every site of its (column, class) pair.
             v += a.wt ? u * a.wt[(size_t)p * d.S + tl.slot0 + q] : u;
         }
         v = warp_sum(v);
-        if (lane == 0) a.partial[tile_id] = v;
+        if (lane == 0 && ek < 0) a.partial[tile_id] = v;
     }
     return tile_ok;
 }
@@ -739,6 +752,8 @@ int prune_default_variant(int R, bool fp32) {
     if (fp32) return 0;
     return R == 4 ? 3 : 1;
 }
+
+bool prune_variant_has_eval(int R, bool fp32, int variant) { return variant < simt_variants(R, fp32); }
 
 int prune_variant_tile_sites(int R, bool fp32, int variant) {
     if (variant < simt_variants(R, fp32)) return 32 * simt_width(R, variant);

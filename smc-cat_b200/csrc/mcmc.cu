@@ -842,6 +842,57 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     int rc = smccat_get_stream(c, &stv);
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stv);
+    // A Gibbs pass evaluates the drawn site under every class at every
+    // iteration. For the classes the particles enter with, those values are
+    // evaluated beforehand for every site in one batched pruning pass per
+    // class (the SIMT pruning kernels' evaluation mode, into the partial
+    // workspaces the committed state does not use) and read from a table.
+    const int pfirst = *std::min_element(list.begin(), list.end());
+    const int prange = *std::max_element(list.begin(), list.end()) - pfirst + 1;
+    DeviceView view;
+    bool use_table = false;
+    if (learned_updates == 0 && site < 0 && device_view(c, pfirst, prange, &view) == SMCCAT_OK)
+        use_table = view.pa.wt == nullptr && prune_variant_has_eval(d.R, view.fp32, view.variant);
+    std::vector<PartHdr> ehdr;
+    std::vector<NodeJob> enodes;
+    std::vector<int32_t> emap;
+    std::vector<uint8_t> esws;
+    int kmax_list = 0;
+    if (use_table) {
+        ehdr.assign(prange, PartHdr{});
+        enodes.assign((size_t)prange * d.NI, NodeJob{0, 0, 0, 0});
+        emap.assign(prange, -1);
+        esws.assign((size_t)prange * d.Kmax, 0);
+        for (int q = 0; q < prange; ++q) {
+            const Mirror& m = slot_of(c, pfirst + q).cur;
+            std::copy(m.sws.begin(), m.sws.end(), &esws[(size_t)q * d.Kmax]);
+        }
+        for (int j = 0; j < n; ++j) {
+            const int q = list[j] - pfirst;
+            const Mirror& m = slot_of(c, list[j]).cur;
+            emap[q] = j;
+            kmax_list = std::max(kmax_list, m.K);
+            PartHdr& h = ehdr[q];
+            h.node_off = q * d.NI;
+            h.node_cnt = (int)m.post.size();
+            h.root = m.root;
+            h.root_ws = 1 - m.clws[m.root];
+            h.active = 1;
+            h.num_classes = m.K;
+            h.cls_only = -1;
+            h.pinv = m.pinv;
+            for (int r = 0; r < kMaxRates; ++r) h.rates[r] = m.rates[r];
+            for (int x = 0; x < (int)m.post.size(); ++x) {
+                const int nd = m.post[x], c1 = m.kids[2 * nd], c2 = m.kids[2 * nd + 1];
+                int ws = 1 - m.clws[nd];
+                if (c1 >= d.T) ws |= (1 - m.clws[c1]) << 1;
+                if (c2 >= d.T) ws |= (1 - m.clws[c2]) << 2;
+                ws |= m.pws[c1] << 3;
+                ws |= m.pws[c2] << 4;
+                enodes[(size_t)q * d.NI + x] = NodeJob{nd, c1, c2, ws};
+            }
+        }
+    }
     // Device buffers for this call (inputs, outputs and kernel scratch).
     const size_t scratch = gibbs_scratch_doubles(d, n, Kcap);
     size_t bytes = 0;
@@ -853,6 +904,13 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
                  o_aux = carve(auxv.size() * 8), o_w = carve((size_t)n * ks * 8),
                  o_status = carve(4), o_scr = carve(scratch * 8), o_acc = carve((size_t)n * 4),
                  o_prop = carve((size_t)n * 4);
+    size_t o_ehdr = 0, o_enodes = 0, o_emap = 0, o_table = 0;
+    if (use_table) {
+        o_ehdr = carve(sizeof(PartHdr) * ehdr.size());
+        o_enodes = carve(sizeof(NodeJob) * enodes.size());
+        o_emap = carve(4 * emap.size());
+        o_table = carve((size_t)n * d.Kmax * d.S * 8);
+    }
     char* dbuf = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&dbuf, bytes, st);
     if (e != cudaSuccess) return mfail(SMCCAT_ENOMEM, std::string("gibbs buffers: ") + cudaGetErrorString(e));
@@ -873,6 +931,25 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     up(o_assign, assign.data(), assign.size() * 4);
     up(o_aux, auxv.data(), auxv.size() * 8);
     if (e == cudaSuccess) e = cudaMemsetAsync(dbuf + o_status, 0, 4, st);
+    if (use_table) {
+        up(o_ehdr, ehdr.data(), sizeof(PartHdr) * ehdr.size());
+        up(o_enodes, enodes.data(), sizeof(NodeJob) * enodes.size());
+        up(o_emap, emap.data(), 4 * emap.size());
+        // The committed workspace bytes (a host-side reject since the last
+        // refresh may have left the device array on the rejected ones).
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(const_cast<uint8_t*>(view.sws) + (size_t)pfirst * d.Kmax, esws.data(),
+                                esws.size(), cudaMemcpyHostToDevice, st);
+        PruneArgs pa = view.pa;
+        pa.hdr = reinterpret_cast<const PartHdr*>(dbuf + o_ehdr);
+        pa.nodes = reinterpret_cast<const NodeJob*>(dbuf + o_enodes);
+        pa.eval_map = reinterpret_cast<const int32_t*>(dbuf + o_emap);
+        pa.eval_out = reinterpret_cast<double*>(dbuf + o_table);
+        for (int k = 0; k < kmax_list && e == cudaSuccess; ++k) {
+            pa.eval_k = k;
+            e = launch_prune(pa, view.ntiles, view.variant, st);
+        }
+    }
     if (e == cudaSuccess) {
         GibbsArgs a{};
         a.d = d;
@@ -895,6 +972,8 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         a.isinv = isinv_device(c);
         a.invchar = invchar_device(c);
         a.status = reinterpret_cast<int*>(dbuf + o_status);
+        a.table = use_table ? reinterpret_cast<const double*>(dbuf + o_table) : nullptr;
+        a.Kt = d.Kmax;
         if (learned_updates > 0)
             e = launch_learned_move(a, mlp, site_feat, reinterpret_cast<int32_t*>(dbuf + o_acc),
                                     reinterpret_cast<int32_t*>(dbuf + o_prop),

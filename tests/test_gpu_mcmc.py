@@ -417,3 +417,32 @@ def test_smc_driver_reaches_temperature_one(reassign):
     for i in range(n):
         assert got[i] == pytest.approx(oracle_lnl_state(codes, CFG, fin, i), rel=1e-9)
     eng.close()
+
+
+def test_gibbs_class_table_matches_per_site_evaluation():
+    """Gibbs reads the site log-likelihoods of the classes a particle enters
+    with from a table the SIMT pruning kernels fill beforehand; with a kernel
+    variant that has no evaluation mode (the FP64 tensor-path kernels) every
+    class is pruned per site inside the Gibbs kernel instead. Same state, same
+    seed: the same draws, hence the same assignments and likelihoods."""
+    cfg = workload.WorkloadConfig("gibbs_table", T=10, S=300, R=4, particles=6, iterations=1,
+                                  lg=False, invar=True, cat=True, pinv=0.1, k_range=(2, 7), seed=71)
+    rng = np.random.default_rng(cfg.seed)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    st = workload.make_particles(cfg, cfg.particles, rng, kmax=24)
+    out = []
+    for variant in (None, "dmma"):
+        eng = smccat.Engine(codes, cfg.R, cfg.particles, max_classes=24, invar=True, cat=True)
+        eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                          st["logits"], st["assign"], st["pinv"], st["shape"])
+        eng.refresh(full=True)
+        if variant == "dmma":
+            n, _ = eng.kernel_variants()
+            eng.set_kernel_variant(n - 1)
+        eng.gibbs(temperature=0.8, seed=13)
+        out.append((eng.get_particles(), eng.lnl()))
+        eng.close()
+    (a, la), (b, lb) = out
+    np.testing.assert_array_equal(a["num_classes"], b["num_classes"])
+    np.testing.assert_array_equal(a["assign"], b["assign"])
+    np.testing.assert_allclose(la, lb, rtol=1e-12)
