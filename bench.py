@@ -75,7 +75,10 @@ def parse():
                     help="CAT config on which to compare sampler sweeps/s and ESS/s: plain FP64 + "
                          "Gibbs against FP32 + device graph sweep + learned proposal (0 to skip)")
     ap.add_argument("--sampler-particles", type=int, default=48)
-    ap.add_argument("--sampler-sweeps", type=int, default=4)
+    ap.add_argument("--sampler-sweeps", type=int, default=4,
+                    help="timed sweeps of the plain arm")
+    ap.add_argument("--sampler-chosen-sweeps", type=int, default=10,
+                    help="timed sweeps of the chosen arm (a whole Gibbs period)")
     ap.add_argument("--smc", type=int, default=0,
                     help="run whole SMC analyses (temperature 0 -> 1) on a 16-taxon x 500-site "
                          "CAT workload: plain FP64 + Gibbs against FP32 + learned proposal, "
@@ -890,7 +893,8 @@ def main():
             line["smc"] = measure_smc(args.smc, args.smc_particles, local, torch)
         if args.sampler_config:
             line["sampler"] = measure_sampler(args.sampler_config, args.sampler_particles,
-                                              args.sampler_sweeps, local, torch)
+                                              args.sampler_sweeps, local, torch,
+                                              chosen_sweeps=args.sampler_chosen_sweeps)
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(cfg, codes, st, args.cpu_sample)
         print(json.dumps(line), flush=True)
