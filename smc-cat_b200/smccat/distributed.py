@@ -156,7 +156,9 @@ def resample_engine(engine, raw_w, target_ess, last_temp, u, group=None, device=
     """One SMC weight step for a sharded population: all-gather the
     log-likelihoods, computeNextStep, and if the ESS fell to the target,
     resample systematically and move the surviving states between ranks,
-    reload them into `engine` and refresh. Returns (raw_w, temp, ess, resampled)."""
+    reload them into `engine` and refresh. Returns (raw_w, temp, ess,
+    resampled) with the raw weights updated to the new temperature; after a
+    resample the caller restarts them at -log N (main.cpp:309)."""
     lnl = all_gather_lnl(engine.lnl(), group, device)
     w, nw, ess, temp = next_step(raw_w, lnl, target_ess, last_temp)
     if not (ess <= target_ess and temp != 1.0):
@@ -169,4 +171,4 @@ def resample_engine(engine, raw_w, target_ess, last_temp, u, group=None, device=
     engine.set_particles(0, new["parent"], new["branch"], new["base"], new["num_classes"],
                          new["logits"], new["assign"], new["pinv"], new["shape"])
     engine.refresh(full=True)
-    return np.full(len(w), -np.log(len(w))), temp, ess, True
+    return w, temp, ess, True

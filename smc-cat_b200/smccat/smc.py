@@ -88,3 +88,51 @@ def run(eng, *, cat: bool, iterations: int = 20, threshold: float = 0.6,
             "seconds": seconds, "final_ess_per_s": float(ess) / seconds,
             "mh_acceptance": moves["accepted"] / max(moves["proposed"], 1),
             "temperatures": [h[0] for h in history]}
+
+
+def run_sharded(eng, *, group=None, device="cpu", cat: bool, iterations: int = 20,
+                threshold: float = 0.6, alg8_probability: float = 0.1, seed: int = 0,
+                max_steps: int = 100000, sync=None) -> dict:
+    """The same loop over a population sharded across ranks (one engine per
+    rank, each holding the same number of particles; torch.distributed set
+    up by the caller). Every rank keeps the global weight vector: the
+    log-likelihoods are all-gathered for computeNextStep, resampling is
+    systematic over the whole population, and the surviving states move
+    between ranks (smccat.distributed.resample_engine); rejuvenation and
+    Gibbs reassignment stay local. The random draws that must agree (the
+    resampling uniform, the Gibbs mask) come from one stream seeded alike on
+    every rank; each rank's moves use its own."""
+    import torch.distributed as dist
+
+    from . import distributed as sd
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    n_local = eng.P
+    n = n_local * world
+    shared = np.random.default_rng(seed)
+    own = np.random.default_rng([seed, rank + 1])
+    raw = np.full(n, -np.log(n))
+    last, log_z = 0.0, 0.0
+    steps = resamples = 0
+    ess = float(n)
+    t0 = time.perf_counter()
+    while last < 1.0 and steps < max_steps:
+        before = _lse(raw)
+        u = float(shared.random())
+        w, temp, ess, resampled = sd.resample_engine(eng, raw, threshold * n, last, u, group, device)
+        log_z += _lse(w) - before
+        steps += 1
+        if np.isnan(ess):
+            raise RuntimeError("NaN ESS: a log-likelihood came out NaN")  # main.cpp:158-174
+        raw = w
+        if resampled:
+            raw = np.full(n, -np.log(n))
+            resamples += 1
+            eng.rejuvenate(iterations=iterations, temperature=temp, seed=int(own.integers(1 << 62)))
+            mask = (shared.random(n) < alg8_probability).astype(np.uint8)[rank * n_local:(rank + 1) * n_local]
+            if cat and mask.any():
+                eng.gibbs(temperature=temp, seed=int(own.integers(1 << 62)), mask=mask)
+        last = temp
+    if sync is not None:
+        sync()
+    return {"log_z": log_z, "steps": steps, "resamples": resamples, "final_ess": float(ess),
+            "seconds": time.perf_counter() - t0}
