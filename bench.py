@@ -332,16 +332,26 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=10, chosen_sweeps=
 
         def sweep(k, timed):
             out = {}
+            t_a = time.perf_counter()
             if chosen:
                 r = eng.mcmc_sweep(iterations=cfg.iterations, temperature=1.0, seed=100 + k)
+                torch.cuda.synchronize()
+                t_b = time.perf_counter()
                 g = eng.learned_move(updates=cfg.S // 2, temperature=1.0, seed=200 + k)
                 out["acc"] = g["accepted"] / max(g["proposed"], 1)
+                torch.cuda.synchronize()
+                t_c = time.perf_counter()
                 if timed and k % gibbs_every == gibbs_every - 1:
                     eng.gibbs(temperature=1.0, seed=300 + k)
                     out["gibbs"] = True
             else:
                 r = eng.rejuvenate(iterations=cfg.iterations, temperature=1.0, seed=100 + k)
+                torch.cuda.synchronize()
+                t_b = t_c = time.perf_counter()
                 eng.gibbs(temperature=1.0, seed=200 + k)
+            torch.cuda.synchronize()
+            t_d = time.perf_counter()
+            out["parts"] = (t_b - t_a, t_c - t_b, t_d - t_c)  # MCMC, learned move, Gibbs
             out["steps"] = r["lockstep_steps"]
             out["mh"] = (sum(r["accepted"]), sum(r["proposed"]))
             return out
@@ -354,6 +364,7 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=10, chosen_sweeps=
         torch.cuda.synchronize()
         traces = {"lnl": [], "tree_length": [], "classes": []}
         secs, steps, acc, mh_a, mh_p, n_gibbs = 0.0, 0, [], 0, 0, 0
+        parts = np.zeros(3)
         nsw = chosen_sweeps if chosen else sweeps
         for k in range(nsw):
             t0 = time.perf_counter()
@@ -361,6 +372,7 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=10, chosen_sweeps=
             torch.cuda.synchronize()
             secs += time.perf_counter() - t0
             steps += o["steps"]
+            parts += np.array(o["parts"])
             mh_a += o["mh"][0]
             mh_p += o["mh"][1]
             n_gibbs += 1 if (not chosen or o.get("gibbs")) else 0
@@ -376,6 +388,8 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=10, chosen_sweeps=
         info.update({"sweeps_per_s": nsw / secs, "seconds_per_sweep": secs / nsw,
                      "lockstep_steps_per_sweep": steps / nsw,
                      "mcmc_acceptance": mh_a / max(mh_p, 1), "gibbs_passes": n_gibbs,
+                     "seconds_per_sweep_in": {"mcmc": parts[0] / nsw, "learned_move": parts[1] / nsw,
+                                              "gibbs": parts[2] / nsw},
                      "ess": ess, "ess_per_s": {k: v / secs for k, v in ess.items()},
                      "mean_lnl_last": float(np.mean(traces["lnl"][-1])),
                      "mean_classes_last": float(np.mean(traces["classes"][-1]))})
