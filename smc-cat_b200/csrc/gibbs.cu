@@ -1,15 +1,21 @@
 // CAT class reassignment (Neal's Algorithm 8, m = 5 auxiliary classes) on the
 // device: Particle::gibbsPartitionMove (Particle.cpp:785-995), corrected form.
 //
-// One CTA per particle runs the floor(S/2) site iterations in order. Each
-// iteration: draw a site and take it out of its class (dropping the class if
-// it empties), draw m fresh classes from the prior (19 N(0,1) logits + 0,
-// TransitionProbabilityClass.cpp:26-35) and diagonalise them (one warp each),
-// evaluate the site's likelihood under every live class and every auxiliary
-// class (one warp per (class, rate) pair, lanes = states, single-site pruning
-// in the eigenbasis P(t)x = L (exp(lambda t) o (Rm x))), weight each class by
-// temperature * log L + log n_k (or log(alpha / m) for the auxiliaries) and
-// draw the new class. Random numbers come from a per-particle Philox stream.
+// Each of the floor(S/2) site iterations of a particle draws a site, takes it
+// out of its class (dropping the class if it empties), draws m fresh classes
+// from the prior (19 N(0,1) logits + 0, TransitionProbabilityClass.cpp:26-35),
+// weights every live class and every auxiliary by temperature * log L +
+// log n_k (or log(alpha / m)) and draws the new class. The drawn sites and the
+// auxiliary classes do not depend on the chain's state, so a pass runs in two
+// kernels: gibbs_aux_kernel diagonalises every iteration's auxiliary classes
+// and prunes their sites, all iterations of all particles at once (one warp per
+// (particle, iteration, auxiliary), lanes = states, single-site pruning in the
+// eigenbasis P(t)x = L (exp(lambda t) o (Rm x))); then gibbs_kernel walks each
+// particle's iterations in order (one CTA per particle) with the site values of
+// the entry classes from a table the pruning kernels fill, those of classes
+// opened during the pass pruned per site, and those of the auxiliaries from
+// the first kernel. Random numbers come from a Philox stream per (particle,
+// iteration).
 //
 // Two reference quirks are not reproduced: its tip read ignores the rate
 // stride (Particle.cpp:895) and its rescalers are written and read at
@@ -29,6 +35,41 @@ namespace {
 
 constexpr int kGibbsWarps = 16;
 constexpr int kAux = 5;
+constexpr int kAuxWarps = 4;  // warps per CTA of the auxiliary-class kernel
+constexpr int kAuxCtasPerSm = 3;
+
+// Random numbers of site iteration `it` of particle p come from the Philox
+// stream (seed, subsequence (p << 24) | it), at fixed offsets (32-bit draws):
+// the site at 0, auxiliary class j's 19 logits at 64 (j + 1), the class draw
+// at 64 (kAux + 1). The auxiliary-class kernel and the sequential pass read
+// the same draws, and no draw depends on the chain's state.
+constexpr unsigned long long kOffAux = 64, kOffChoice = 64ull * (kAux + 1);
+
+__device__ __forceinline__ unsigned long long iter_stream(int p, int it) {
+    return ((unsigned long long)p << 24) | (unsigned long long)it;
+}
+
+__device__ int draw_site(unsigned long long seed, int p, int it, int S) {
+    curandStatePhilox4_32_10_t r;
+    curand_init(seed, iter_stream(p, it), 0ull, &r);
+    const double u = curand_uniform_double(&r);  // (0, 1]
+    const int s = (int)((1.0 - u) * S);
+    return s < S ? s : S - 1;
+}
+
+// 19 N(0,1) logits and a 0 (TransitionProbabilityClass.cpp:26-35).
+__device__ void draw_aux_logits(unsigned long long seed, int p, int it, int j, double* out) {
+    curandStatePhilox4_32_10_t r;
+    curand_init(seed, iter_stream(p, it), kOffAux + 64ull * j, &r);
+    for (int m = 0; m < kStates - 1; ++m) out[m] = curand_normal_double(&r);
+    out[kStates - 1] = 0.0;
+}
+
+__device__ double draw_choice(unsigned long long seed, int p, int it) {
+    curandStatePhilox4_32_10_t r;
+    curand_init(seed, iter_stream(p, it), kOffChoice, &r);
+    return curand_uniform_double(&r);
+}
 
 __device__ __forceinline__ double warp_max20(double v) {
 #pragma unroll
@@ -42,15 +83,21 @@ __device__ __forceinline__ double wsum(double v) {
     return v;
 }
 
-// exp(lambda_m t_n r) for every (node, rate) of class slot k.
-__device__ void fill_exp(const GibbsArgs& a, int i, int k, const double* rec, double* ex) {
-    const Dims& d = a.d;
-    const GibbsPart& gp = a.parts[i];
-    const double* br = a.branch + (size_t)i * d.N;
-    for (int idx = threadIdx.x; idx < d.N * d.R * kStates; idx += blockDim.x) {
-        const int m = idx % kStates, r = (idx / kStates) % d.R, n = idx / (kStates * d.R);
-        ex[idx] = exp(rec[kSpecLam + m] * br[n] * gp.rates[r]);
+__device__ __forceinline__ float warp_maxf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Inclusive prefix sum over the warp's lanes.
+__device__ __forceinline__ double warp_incl_scan(double x) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
     }
+    return x;
 }
 
 // Rates per warp in the Gibbs weights (all of a class's rates together) and in
@@ -60,16 +107,17 @@ constexpr int kRateBlockLearned = 2;
 
 // Log-likelihoods of one site under one class for rates [r0, r0 + RB) (those
 // below R), one warp: lanes are states and the rate chains interleave.
-// Single-site pruning in the eigenbasis, P(t r) x = L (exp(lambda t r) o (Rm x)).
-// The vectors every lane needs whole (x before Rm, z before L) pass through the
-// warp's shared exchange row `xch` [RB][kStates] and are read back as broadcast
-// pairs, not shuffled lane by lane. The node computed last stays in registers
-// (in post-order it is a child of the next node); other internal children come
-// back from the warp's stash [NI][RB][32]. Tip codes of the site come from
+// Single-site pruning in the eigenbasis, P(t r) x = L (exp(lambda t r) o (Rm x)),
+// with exp(lambda_m t r) evaluated where it is used. The vectors every lane
+// needs whole (x before Rm, z before L) pass through the warp's shared
+// exchange row `xch` [RB][kStates] and are read back as broadcast pairs, not
+// shuffled lane by lane. The node computed last stays in registers (in
+// post-order it is a child of the next node); other internal children come
+// back from the warp's stash [nslots][RB][32]. Tip codes of the site come from
 // `scode` (shared). out[b] = log L of rate r0 + b.
 template <int RB>
-__device__ void site_class_lnl(const GibbsArgs& a, int i, int r0, const double* rec,
-                               const double* ex, double* stash, const uint8_t* scode,
+__device__ void site_class_lnl(const GibbsArgs& a, const GibbsPart& gp, int i, int r0,
+                               const double* rec, double* stash, const uint8_t* scode,
                                double* xch, double* out) {
     using D2 = double2;
     const Dims& d = a.d;
@@ -82,31 +130,34 @@ __device__ void site_class_lnl(const GibbsArgs& a, int i, int r0, const double* 
         Lrow[m] = rec[kSpecL + li * kStates + m];   // L[lane][m]
         Rrow[m] = rec[kSpecRm + li * kStates + m];  // Rm[lane][m]
     }
+    const double lam = rec[kSpecLam + li];
     double rs = 0.0;
 #pragma unroll
     for (int j = 0; j < kStates; ++j) rs += Rrow[j];
     bool on[RB];
-    double v[RB], lsc[RB];
+    double v[RB], lsc[RB], rate[RB];
 #pragma unroll
     for (int b = 0; b < RB; ++b) {
         on[b] = r0 + b < d.R;
+        rate[b] = on[b] ? gp.rates[r0 + b] : 0.0;
         v[b] = 1.0;
         lsc[b] = 0.0;
     }
-    const int32_t* tree = a.tree + (size_t)i * d.NI * 3;
+    const GibbsNode* tree = a.nodes + (size_t)i * d.NI;
+    const double* br = a.branch + (size_t)i * d.N;
     int prev = -1;
     for (int q = 0; q < d.NI; ++q) {
-        const int n = tree[3 * q];
+        const GibbsNode nd = tree[q];
         double vn[RB];
 #pragma unroll
         for (int b = 0; b < RB; ++b) vn[b] = 1.0;
 #pragma unroll 1
-        for (int ci = 1; ci <= 2; ++ci) {
-            const int c = tree[3 * q + ci];
+        for (int ci = 0; ci < 2; ++ci) {
+            const int c = nd.c[ci];
+            const double lt = lam * br[c];
             double e[RB], z[RB];
 #pragma unroll
-            for (int b = 0; b < RB; ++b)
-                e[b] = on[b] ? ex[((size_t)c * d.R + r0 + b) * kStates + li] : 0.0;
+            for (int b = 0; b < RB; ++b) e[b] = on[b] ? exp(lt * rate[b]) : 0.0;
             if (c < d.T) {
                 const int code = scode[c];
                 double rc = rs;
@@ -117,10 +168,10 @@ __device__ void site_class_lnl(const GibbsArgs& a, int i, int r0, const double* 
 #pragma unroll
                 for (int b = 0; b < RB; ++b) z[b] = e[b] * rc;
             } else {
+                const double* sx = stash + (size_t)nd.sc[ci] * RB * 32;
 #pragma unroll
                 for (int b = 0; b < RB; ++b) {
-                    const double xv = (c == prev) ? v[b]
-                                                  : stash[((size_t)(c - d.T) * RB + b) * 32 + lane];
+                    const double xv = (c == prev) ? v[b] : sx[b * 32 + lane];
                     if (st_lane) xch[b * kStates + lane] = xv;
                 }
                 __syncwarp();
@@ -160,6 +211,7 @@ __device__ void site_class_lnl(const GibbsArgs& a, int i, int r0, const double* 
 #pragma unroll
             for (int b = 0; b < RB; ++b) vn[b] *= y[b];
         }
+        double* so = stash + (size_t)nd.so * RB * 32;
 #pragma unroll
         for (int b = 0; b < RB; ++b) {
             double x = st_lane ? vn[b] : 0.0;
@@ -173,9 +225,9 @@ __device__ void site_class_lnl(const GibbsArgs& a, int i, int r0, const double* 
                 lsc[b] = -INFINITY;
             }
             v[b] = x;
-            stash[((size_t)(n - d.T) * RB + b) * 32 + lane] = x;
+            so[b * 32 + lane] = x;
         }
-        prev = n;
+        prev = nd.n;
         __syncwarp();
     }
     const double pi = st_lane ? rec[kSpecPi + lane] : 0.0;
@@ -186,37 +238,115 @@ __device__ void site_class_lnl(const GibbsArgs& a, int i, int r0, const double* 
     }
 }
 
+// Site log-likelihood (+I mixed) from the per-rate values l[r]
+// (Particle.cpp:931-950, corrected form).
+__device__ double site_value(const GibbsArgs& a, const GibbsPart& gp, int s, const double* l,
+                             const double* pi) {
+    double mx = -INFINITY;
+    for (int r = 0; r < a.d.R; ++r) mx = fmax(mx, l[r]);
+    double lse = mx;
+    if (mx > -INFINITY) {
+        double se = 0.0;
+        for (int r = 0; r < a.d.R; ++r) se += exp(l[r] - mx);
+        lse = mx + log(se);
+    }
+    if (gp.pinv > 0.0 && a.isinv[s] != 0) {
+        const double la = log1p(-gp.pinv) + lse;
+        const double lb = log(gp.pinv * pi[a.invchar[s]]);
+        const double m2 = fmax(la, lb);
+        return m2 + log(exp(la - m2) + exp(lb - m2));
+    }
+    return lse + log1p(-gp.pinv);
+}
+
+// Every iteration's drawn site and its log-likelihood under each of the m
+// auxiliary classes (Particle.cpp:823-833 and :857-930 for the auxiliaries),
+// for all particles and iterations at once: one warp per (particle,
+// iteration, auxiliary class) draws the site and the class's logits,
+// diagonalises the class and prunes the site. In weights mode the site is the
+// fixed one and the logits come from aux_in.
+__global__ void __launch_bounds__(32 * kAuxWarps, kAuxCtasPerSm) gibbs_aux_kernel(GibbsArgs a, int n_iter) {
+    const Dims& d = a.d;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ SpecWork work[kAuxWarps];
+    __shared__ __align__(16) double xch[kAuxWarps][kRateBlock * kStates];
+    __shared__ double lg[kAuxWarps][kStates];
+    __shared__ double lr[kAuxWarps][kMaxRates];
+    __shared__ int ssite[kAuxWarps];
+    extern __shared__ uint8_t scodes[];  // [kAuxWarps][T]
+    uint8_t* scode = scodes + (size_t)warp * d.T;
+    const size_t gw = (size_t)blockIdx.x * kAuxWarps + warp;
+    double* rec = a.aux_rec + gw * kSpecStride;
+    double* stash = a.aux_stash + gw * a.nslots * kRateBlock * 32;
+    const size_t tasks = (size_t)a.count * n_iter * kAux;
+    for (size_t t = gw; t < tasks; t += (size_t)gridDim.x * kAuxWarps) {
+        const int j = (int)(t % kAux);
+        const size_t ii = t / kAux;  // particle * n_iter + iteration
+        const int it = (int)(ii % n_iter), i = (int)(ii / n_iter);
+        const GibbsPart& gp = a.parts[i];
+        if (lane == 0) {
+            int s;
+            if (gp.fixed_site >= 0) {
+                s = gp.fixed_site;
+                for (int m = 0; m < kStates; ++m) lg[warp][m] = a.aux_in[((size_t)i * kAux + j) * kStates + m];
+            } else {
+                s = draw_site(a.seed, gp.p, it, d.S);
+                draw_aux_logits(a.seed, gp.p, it, j, lg[warp]);
+            }
+            ssite[warp] = s;
+            if (j == 0) a.aux_site[ii] = s;
+        }
+        __syncwarp();
+        const int s = ssite[warp];
+        for (int c = lane; c < d.T; c += 32) scode[c] = a.codes[(size_t)c * d.S + s];
+        spectral_decompose_warp_ws(a.base + (size_t)i * kBase, lg[warp], rec, work[warp]);
+        __syncwarp();
+        for (int r0 = 0; r0 < d.R; r0 += kRateBlock)
+            site_class_lnl<kRateBlock>(a, gp, i, r0, rec, stash, scode, xch[warp], lr[warp] + r0);
+        __syncwarp();
+        if (lane == 0) a.aux_ls[t] = site_value(a, gp, s, lr[warp], rec + kSpecPi);
+        __syncwarp();
+    }
+}
+
+// The sequential part of a Gibbs pass, one CTA per particle over its
+// iterations in order. Each iteration takes the drawn site out of its class
+// (dropping the class if it empties), weights every live class by
+// temperature * log L + log n_k and each auxiliary by temperature * log L +
+// log(alpha / m), and draws the new class. A class's log L comes from the
+// table (the classes the particle entered with), from single-site pruning
+// (classes opened during this pass, one warp per class, all its rates
+// together), or from the auxiliary-class kernel. An auxiliary that is drawn
+// becomes class slot kcur: its logits are drawn again from the same stream
+// and it is diagonalised once.
 __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
     const Dims& d = a.d;
     const int i = blockIdx.x;
     const GibbsPart gp = a.parts[i];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int Kcap = a.Kcap;
-    double* spec = a.spec + (size_t)i * (Kcap + kAux) * kSpecStride;
-    double* ex = a.expt + (size_t)i * (Kcap + kAux) * d.N * d.R * kStates;
-    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * d.NI * kRateBlock * 32;
+    double* spec = a.spec + (size_t)i * Kcap * kSpecStride;
+    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * a.nslots * kRateBlock * 32;
     __shared__ __align__(16) double xch[kGibbsWarps][kRateBlock * kStates];
     double* logits = a.logits + (size_t)i * (Kcap + kAux) * kStates;
     int32_t* assign = a.assign + (size_t)i * d.S;
     const double* base = a.base + (size_t)i * kBase;
-    extern __shared__ double sh[];                   // lnl [(Kcap + kAux) * R]
-    double* wts = sh + (size_t)(Kcap + kAux) * d.R;  // [Kcap + kAux]
+    extern __shared__ double sh[];                   // lnl [Kcap * R]
+    double* wts = sh + (size_t)Kcap * d.R;           // [Kcap + kAux]
     int* counts = reinterpret_cast<int*>(wts + (Kcap + kAux));  // [Kcap + kAux]
     uint8_t* scode = reinterpret_cast<uint8_t*>(counts + (Kcap + kAux));  // [T]: the site's column
     const bool weights_mode = gp.fixed_site >= 0;
     __shared__ int s_site, s_kcur, s_choice;
     __shared__ SpecWork work[kAux];
-    __shared__ curandStatePhilox4_32_10_t rng_state;
+    const double* auxl = a.aux_ls + (size_t)i * gp.n_iter * kAux;
+    const int32_t* auxs = a.aux_site + (size_t)i * gp.n_iter;
 
-    if (threadIdx.x == 0) {
-        curand_init(a.seed, (unsigned long long)gp.p, 0ull, &rng_state);
-        s_kcur = gp.K;
-    }
+    if (threadIdx.x == 0) s_kcur = gp.K;
     for (int k = threadIdx.x; k < Kcap + kAux; k += blockDim.x) counts[k] = 0;
     __syncthreads();
     for (int x = threadIdx.x; x < d.S; x += blockDim.x) atomicAdd(&counts[assign[x]], 1);
     // Classes [0, K0) read their site log-likelihoods from the table; the
-    // others (none without a table) are pruned per site below.
+    // others (all of them without a table) are pruned per site below.
     const int K0 = a.table ? gp.K : 0;
     const double* tab = a.table ? a.table + (size_t)i * a.Kt * d.S : nullptr;
     if (warp < kAux)  // one shared workspace per decomposing warp
@@ -224,128 +354,99 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
             spectral_decompose_warp_ws(base, logits + (size_t)k * kStates,
                                        spec + (size_t)k * kSpecStride, work[warp]);
     __syncthreads();
-    for (int k = K0; k < gp.K; ++k)
-        fill_exp(a, i, k, spec + (size_t)k * kSpecStride, ex + (size_t)k * d.N * d.R * kStates);
-    __syncthreads();
 
     const double alpha_split = log(a.alpha / kAux);
     for (int it = 0; it < gp.n_iter; ++it) {
-        // 1. draw the site and remove it from its class (Particle.cpp:808-821)
+        // 1. the drawn site leaves its class (Particle.cpp:808-821)
         if (threadIdx.x == 0) {
-            int s;
-            if (weights_mode) {
-                s = gp.fixed_site;
-            } else {
-                const double u = curand_uniform_double(&rng_state);  // (0, 1]
-                s = (int)((1.0 - u) * d.S);
-                s = s < d.S ? s : d.S - 1;
-            }
+            const int s = auxs[it];
             s_site = s;
             counts[assign[s]]--;
-            for (int j = 0; j < kAux; ++j)
-                for (int m = 0; m < kStates; ++m)
-                    logits[(size_t)(s_kcur + j) * kStates + m] =
-                        weights_mode ? a.aux_in[((size_t)i * kAux + j) * kStates + m]
-                                     : ((m < kStates - 1) ? curand_normal_double(&rng_state) : 0.0);
         }
         __syncthreads();
         const int s = s_site, kcur = s_kcur;
-        for (int c = threadIdx.x; c < d.T; c += blockDim.x) scode[c] = a.codes[(size_t)c * d.S + s];
-        // 2. diagonalise the auxiliary classes (Particle.cpp:823-833)
-        if (warp < kAux)
-            spectral_decompose_warp_ws(base, logits + (size_t)(kcur + warp) * kStates,
-                                       spec + (size_t)(kcur + warp) * kSpecStride, work[warp]);
-        __syncthreads();
-        for (int j = 0; j < kAux; ++j)
-            fill_exp(a, i, kcur + j, spec + (size_t)(kcur + j) * kSpecStride,
-                     ex + (size_t)(kcur + j) * d.N * d.R * kStates);
-        __syncthreads();
-        // 3. site log-likelihood per (class, rate) (Particle.cpp:857-930): one
-        // warp per class, all its rates together
-        for (int k = K0 + warp; k < kcur + kAux; k += kGibbsWarps) {
-            if (k >= kcur || counts[k] > 0) {
-                for (int r0 = 0; r0 < d.R; r0 += kRateBlock)
-                    site_class_lnl<kRateBlock>(a, i, r0, spec + (size_t)k * kSpecStride,
-                                               ex + (size_t)k * d.N * d.R * kStates, stash, scode,
-                                               xch[warp], sh + (size_t)k * d.R + r0);
-            } else if (lane == 0) {
-                for (int r = 0; r < d.R; ++r) sh[(size_t)k * d.R + r] = -INFINITY;
-            }
+        // 2. per-site pruning of the classes not in the table (Particle.cpp:857-930)
+        if (kcur > K0) {
+            for (int c = threadIdx.x; c < d.T; c += blockDim.x) scode[c] = a.codes[(size_t)c * d.S + s];
+            __syncthreads();
+            for (int k = K0 + warp; k < kcur; k += kGibbsWarps)
+                if (counts[k] > 0)
+                    for (int r0 = 0; r0 < d.R; r0 += kRateBlock)
+                        site_class_lnl<kRateBlock>(a, gp, i, r0, spec + (size_t)k * kSpecStride, stash,
+                                                   scode, xch[warp], sh + (size_t)k * d.R + r0);
+            __syncthreads();
         }
-        __syncthreads();
-        // 4. weights and the draw (Particle.cpp:931-978)
-        if (threadIdx.x == 0) {
+        // 3. weights and the draw (Particle.cpp:931-978), one warp: lanes take
+        // classes in turn; the cumulative sum runs in class order, chunk by
+        // chunk of 32 with a warp scan, and the total is that sum's end.
+        if (warp == 0) {
+            const int ktot = kcur + kAux;
             double wmax = -INFINITY;
-            for (int k = 0; k < kcur + kAux; ++k) {
+            for (int k = lane; k < ktot; k += 32) {
                 double w = -INFINITY;
-                if (k < K0 && counts[k] > 0) {
-                    w = tab[(size_t)k * d.S + s] * a.temp + log((double)counts[k]);
-                } else if (k >= kcur || counts[k] > 0) {
-                    double mx = -INFINITY;
-                    for (int r = 0; r < d.R; ++r) mx = fmax(mx, sh[k * d.R + r]);
-                    double lse = mx;
-                    if (mx > -INFINITY) {
-                        double se = 0.0;
-                        for (int r = 0; r < d.R; ++r) se += exp(sh[k * d.R + r] - mx);
-                        lse = mx + log(se);
-                    }
-                    const double* pi = spec + (size_t)k * kSpecStride + kSpecPi;
-                    double ls;
-                    if (gp.pinv > 0.0 && a.isinv[s] != 0) {
-                        const double la = log1p(-gp.pinv) + lse;
-                        const double lb = log(gp.pinv * pi[a.invchar[s]]);
-                        const double m2 = fmax(la, lb);
-                        ls = m2 + log(exp(la - m2) + exp(lb - m2));
-                    } else {
-                        ls = lse + log1p(-gp.pinv);
-                    }
-                    w = ls * a.temp + ((k < kcur) ? log((double)counts[k]) : alpha_split);
+                if (k >= kcur) {
+                    w = auxl[(size_t)it * kAux + (k - kcur)] * a.temp + alpha_split;
+                } else if (counts[k] > 0) {
+                    const double ls = k < K0 ? tab[(size_t)k * d.S + s]
+                                             : site_value(a, gp, s, sh + (size_t)k * d.R,
+                                                          spec + (size_t)k * kSpecStride + kSpecPi);
+                    w = ls * a.temp + log((double)counts[k]);
                 }
                 wts[k] = w;
                 wmax = fmax(wmax, w);
             }
-            if (weights_mode) {
-                for (int k = 0; k < kcur + kAux; ++k)
-                    a.weights_out[(size_t)i * (Kcap + kAux) + k] = wts[k];
-                counts[assign[s]]++;  // leave the state as it was
-            }
-            double tot = 0.0;
-            for (int k = 0; k < kcur + kAux; ++k) tot += exp(wts[k] - wmax);
-            const double draw = tot * curand_uniform_double(&rng_state);
+            wmax = warp_max20(wmax);
+            __syncwarp();
+            if (weights_mode)
+                for (int k = lane; k < ktot; k += 32) a.weights_out[(size_t)i * (Kcap + kAux) + k] = wts[k];
             double run = 0.0;
-            int choice = kcur + kAux - 1;
-            for (int k = 0; k < kcur + kAux; ++k) {
-                const double w = wts[k];
-                if (w == -INFINITY) continue;
-                run += exp(w - wmax);
-                if (run >= draw) { choice = k; break; }
+            for (int b0 = 0; b0 < ktot; b0 += 32) {
+                const int k = b0 + lane;
+                const double x = warp_incl_scan((k < ktot && wts[k] > -INFINITY) ? exp(wts[k] - wmax) : 0.0);
+                run += __shfl_sync(0xffffffffu, x, 31);
             }
-            if (choice >= kcur && kcur >= Kcap) {
-                atomicOr(a.status, 4);  // class capacity exhausted: keep the old class
-                choice = assign[s];
+            const double u = __shfl_sync(0xffffffffu, lane == 0 ? draw_choice(a.seed, gp.p, it) : 0.0, 0);
+            const double draw = run * u;
+            int choice = ktot - 1;
+            run = 0.0;
+            for (int b0 = 0; b0 < ktot; b0 += 32) {
+                const int k = b0 + lane;
+                const bool live = k < ktot && wts[k] > -INFINITY;
+                const double x = warp_incl_scan(live ? exp(wts[k] - wmax) : 0.0);
+                const unsigned hit = __ballot_sync(0xffffffffu, live && run + x >= draw);
+                if (hit) {
+                    choice = b0 + __ffs(hit) - 1;
+                    break;
+                }
+                run += __shfl_sync(0xffffffffu, x, 31);
             }
-            if (weights_mode) choice = -1;
-            s_choice = choice;
+            if (lane == 0) {
+                if (choice >= kcur && kcur >= Kcap) {
+                    atomicOr(a.status, 4);  // class capacity exhausted: keep the old class
+                    choice = assign[s];
+                }
+                if (weights_mode) {
+                    counts[assign[s]]++;  // leave the state as it was
+                    choice = -1;
+                }
+                s_choice = choice;
+            }
         }
         __syncthreads();
         const int choice = s_choice;
         if (choice < 0) break;  // weights mode: nothing changes
         if (choice >= kcur) {
-            // The chosen auxiliary becomes class slot kcur.
-            const int src = choice;
-            if (src != kcur) {
-                for (int x = threadIdx.x; x < kSpecStride; x += blockDim.x)
-                    spec[(size_t)kcur * kSpecStride + x] = spec[(size_t)src * kSpecStride + x];
-                for (int x = threadIdx.x; x < kStates; x += blockDim.x)
-                    logits[(size_t)kcur * kStates + x] = logits[(size_t)src * kStates + x];
-                for (int x = threadIdx.x; x < d.N * d.R * kStates; x += blockDim.x)
-                    ex[(size_t)kcur * d.N * d.R * kStates + x] = ex[(size_t)src * d.N * d.R * kStates + x];
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                assign[s] = kcur;
-                counts[kcur] = 1;
-                s_kcur = kcur + 1;
+            // The drawn auxiliary becomes class slot kcur.
+            if (warp == 0) {
+                if (lane == 0) draw_aux_logits(a.seed, gp.p, it, choice - kcur, logits + (size_t)kcur * kStates);
+                __syncwarp();
+                spectral_decompose_warp_ws(base, logits + (size_t)kcur * kStates,
+                                           spec + (size_t)kcur * kSpecStride, work[0]);
+                if (lane == 0) {
+                    assign[s] = kcur;
+                    counts[kcur] = 1;
+                    s_kcur = kcur + 1;
+                }
             }
         } else if (threadIdx.x == 0) {
             assign[s] = choice;
@@ -404,26 +505,6 @@ __device__ void mlp_features(const float* sf, const double* pi, int n, float* x)
     __syncwarp();
 }
 
-// Tempered, +I-mixed site log-likelihood from per-rate values l[r].
-__device__ double site_value(const GibbsArgs& a, const GibbsPart& gp, int s, const double* l,
-                             const double* pi) {
-    double mx = -INFINITY;
-    for (int r = 0; r < a.d.R; ++r) mx = fmax(mx, l[r]);
-    double lse = mx;
-    if (mx > -INFINITY) {
-        double se = 0.0;
-        for (int r = 0; r < a.d.R; ++r) se += exp(l[r] - mx);
-        lse = mx + log(se);
-    }
-    if (gp.pinv > 0.0 && a.isinv[s] != 0) {
-        const double la = log1p(-gp.pinv) + lse;
-        const double lb = log(gp.pinv * pi[a.invchar[s]]);
-        const double m2 = fmax(la, lb);
-        return m2 + log(exp(la - m2) + exp(lb - m2));
-    }
-    return lse + log1p(-gp.pinv);
-}
-
 __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArgs a,
                                                                         const __nv_bfloat16* mlp,
                                                                         const float* site_feat,
@@ -433,9 +514,12 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
     const GibbsPart gp = a.parts[i];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int K = gp.K;
-    double* spec = a.spec + (size_t)i * (a.Kcap + kAux) * kSpecStride;
-    double* ex = a.expt + (size_t)i * (a.Kcap + kAux) * d.N * d.R * kStates;
-    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * d.NI * kRateBlockLearned * 32;
+    double* spec = a.spec + (size_t)i * a.Kcap * kSpecStride;
+    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * a.nslots * kRateBlockLearned * 32;
+    // With the class table the two classes' site values are looked up;
+    // without it they are pruned per update.
+    const bool tabled = a.table != nullptr;
+    const double* tab = tabled ? a.table + (size_t)i * a.Kt * d.S : nullptr;
     __shared__ __align__(16) double xch[kGibbsWarps][kRateBlockLearned * kStates];
     const double* logits = a.logits + (size_t)i * (a.Kcap + kAux) * kStates;
     int32_t* assign = a.assign + (size_t)i * d.S;
@@ -467,9 +551,6 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
             spectral_decompose_warp_ws(base, logits + (size_t)k * kStates, spec + (size_t)k * kSpecStride,
                                        work[warp]);
     __syncthreads();
-    for (int k = 0; k < K; ++k)
-        fill_exp(a, i, k, spec + (size_t)k * kSpecStride, ex + (size_t)k * d.N * d.R * kStates);
-    __syncthreads();
     for (int it = 0; it < gp.n_iter; ++it) {
         // One site, uniform over all S. A site alone in its class stays put
         // (the move never empties a class), so the site is selected with
@@ -484,7 +565,8 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
         __syncthreads();
         const int s = s_site;
         if (s < 0) continue;
-        for (int c = threadIdx.x; c < d.T; c += blockDim.x) scode[c] = a.codes[(size_t)c * d.S + s];
+        if (!tabled)
+            for (int c = threadIdx.x; c < d.T; c += blockDim.x) scode[c] = a.codes[(size_t)c * d.S + s];
         const float* sf = site_feat + (size_t)s * kSiteFeat;
         for (int k = warp; k < K; k += kGibbsWarps) {  // forward scores
             mlp_features(sf, spec + (size_t)k * kSpecStride + kSpecPi, counts[k], xs + warp * kMlpIn);
@@ -493,21 +575,35 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
             __syncwarp();
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (warp == 0) {  // the proposal draw, in class order (warp scan over chunks of 32)
             float mx = -INFINITY;
-            for (int k = 0; k < K; ++k) mx = fmaxf(mx, score[k]);
-            double tot = 0.0;
-            for (int k = 0; k < K; ++k) tot += exp((double)(score[k] - mx));
-            const double draw = tot * curand_uniform_double(&rng_state);
+            for (int k = lane; k < K; k += 32) mx = fmaxf(mx, score[k]);
+            mx = warp_maxf(mx);
             double run = 0.0;
-            int b = K - 1;
-            for (int k = 0; k < K; ++k) {
-                run += exp((double)(score[k] - mx));
-                if (run >= draw) { b = k; break; }
+            for (int b0 = 0; b0 < K; b0 += 32) {
+                const int k = b0 + lane;
+                const double x = warp_incl_scan(k < K ? exp((double)(score[k] - mx)) : 0.0);
+                run += __shfl_sync(0xffffffffu, x, 31);
             }
-            s_a = assign[s];
-            s_b = b;
-            prop_n++;
+            const double u = __shfl_sync(0xffffffffu, lane == 0 ? curand_uniform_double(&rng_state) : 0.0, 0);
+            const double draw = run * u;
+            int b = K - 1;
+            run = 0.0;
+            for (int b0 = 0; b0 < K; b0 += 32) {
+                const int k = b0 + lane;
+                const double x = warp_incl_scan(k < K ? exp((double)(score[k] - mx)) : 0.0);
+                const unsigned hit = __ballot_sync(0xffffffffu, k < K && run + x >= draw);
+                if (hit) {
+                    b = b0 + __ffs(hit) - 1;
+                    break;
+                }
+                run += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (lane == 0) {
+                s_a = assign[s];
+                s_b = b;
+                prop_n++;
+            }
         }
         __syncthreads();
         const int ca = s_a, cb = s_b;
@@ -516,15 +612,14 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
             __syncthreads();
             continue;
         }
-        // Site likelihoods under the two classes (warps 0..nb-1: a, nb..2nb-1:
-        // b, kRateBlockLearned rates each), reverse scores with the updated
-        // class sizes (warps 2nb, 2nb+1).
-        const int nb = (d.R + kRateBlockLearned - 1) / kRateBlockLearned;
+        // Without the table: site likelihoods under the two classes (warps
+        // 0..nb-1: a, nb..2nb-1: b, kRateBlockLearned rates each). Reverse
+        // scores with the updated class sizes on the next two warps.
+        const int nb = tabled ? 0 : (d.R + kRateBlockLearned - 1) / kRateBlockLearned;
         if (warp < 2 * nb) {
             const int which = warp < nb ? 0 : 1, r0 = (warp % nb) * kRateBlockLearned;
             const int k = which == 0 ? ca : cb;
-            site_class_lnl<kRateBlockLearned>(a, i, r0, spec + (size_t)k * kSpecStride,
-                                              ex + (size_t)k * d.N * d.R * kStates, stash, scode,
+            site_class_lnl<kRateBlockLearned>(a, gp, i, r0, spec + (size_t)k * kSpecStride, stash, scode,
                                               xch[warp], lrate[which] + r0);
         } else if (warp < 2 * nb + 2) {
             const int w = warp - 2 * nb;
@@ -535,29 +630,37 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
             if (lane == 0) rev[w] = v;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            const double la = site_value(a, gp, s, lrate[0], spec + (size_t)ca * kSpecStride + kSpecPi);
-            const double lb = site_value(a, gp, s, lrate[1], spec + (size_t)cb * kSpecStride + kSpecPi);
+        if (warp == 0) {
             float mx = -INFINITY, mx2 = -INFINITY;
-            for (int k = 0; k < K; ++k) {
+            for (int k = lane; k < K; k += 32) {
                 mx = fmaxf(mx, score[k]);
                 mx2 = fmaxf(mx2, k == ca ? rev[0] : (k == cb ? rev[1] : score[k]));
             }
+            mx = warp_maxf(mx);
+            mx2 = warp_maxf(mx2);
             double z = 0.0, z2 = 0.0;
-            for (int k = 0; k < K; ++k) {
+            for (int k = lane; k < K; k += 32) {
                 z += exp((double)(score[k] - mx));
                 z2 += exp((double)((k == ca ? rev[0] : (k == cb ? rev[1] : score[k])) - mx2));
             }
-            const double lq_fwd = (score[cb] - mx) - log(z);
-            const double lq_rev = (rev[0] - mx2) - log(z2);
-            // CRP prior ratio n_b / (n_a - 1); tempered likelihood ratio.
-            const double lr = a.temp * (lb - la) + log((double)counts[cb]) - log((double)(counts[ca] - 1)) +
-                              lq_rev - lq_fwd;
-            if (log(curand_uniform_double(&rng_state)) <= lr) {
-                assign[s] = cb;
-                counts[ca]--;
-                counts[cb]++;
-                acc_n++;
+            z = wsum(z);
+            z2 = wsum(z2);
+            if (lane == 0) {
+                const double la = tabled ? tab[(size_t)ca * d.S + s]
+                                         : site_value(a, gp, s, lrate[0], spec + (size_t)ca * kSpecStride + kSpecPi);
+                const double lb = tabled ? tab[(size_t)cb * d.S + s]
+                                         : site_value(a, gp, s, lrate[1], spec + (size_t)cb * kSpecStride + kSpecPi);
+                const double lq_fwd = (score[cb] - mx) - log(z);
+                const double lq_rev = (rev[0] - mx2) - log(z2);
+                // CRP prior ratio n_b / (n_a - 1); tempered likelihood ratio.
+                const double lr = a.temp * (lb - la) + log((double)counts[cb]) -
+                                  log((double)(counts[ca] - 1)) + lq_rev - lq_fwd;
+                if (log(curand_uniform_double(&rng_state)) <= lr) {
+                    assign[s] = cb;
+                    counts[ca]--;
+                    counts[cb]++;
+                    acc_n++;
+                }
             }
         }
         __syncthreads();
@@ -572,12 +675,53 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
 
 }  // namespace
 
-cudaError_t launch_learned_move(GibbsArgs a, const void* mlp, const float* site_feat, int32_t* n_acc,
-                                int32_t* n_prop, double* scratch, cudaStream_t st) {
+namespace {
+
+// Grid of the auxiliary-class kernel: kAuxCtasPerSm CTAs per SM, or fewer
+// when there are fewer tasks.
+int aux_grid(size_t tasks) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+            sms = 148;
+    }
+    const size_t want = (tasks + kAuxWarps - 1) / kAuxWarps;
+    const size_t cap = (size_t)sms * kAuxCtasPerSm;
+    return (int)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
+struct ScratchLayout {
+    size_t spec, stash, aux_ls, aux_site, aux_rec, aux_stash, total;
+};
+
+ScratchLayout scratch_layout(const Dims& d, int count, int Kcap, int n_iter, int nslots, bool aux) {
+    ScratchLayout L{};
+    size_t o = 0;
+    auto take = [&](size_t n) { const size_t r = o; o += (n + 31) & ~size_t(31); return r; };
+    L.spec = take((size_t)count * Kcap * kSpecStride);
+    L.stash = take((size_t)count * kGibbsWarps * nslots * kRateBlock * 32);
+    if (aux) {
+        const size_t tasks = (size_t)count * n_iter * kAux;
+        const size_t warps = (size_t)aux_grid(tasks) * kAuxWarps;
+        L.aux_ls = take(tasks);
+        L.aux_site = take(((size_t)count * n_iter + 1) / 2);  // int32 pairs
+        L.aux_rec = take(warps * kSpecStride);
+        L.aux_stash = take(warps * nslots * kRateBlock * 32);
+    }
+    L.total = o;
+    return L;
+}
+
+}  // namespace
+
+cudaError_t launch_learned_move(GibbsArgs a, int n_iter, const void* mlp, const float* site_feat,
+                                int32_t* n_acc, int32_t* n_prop, double* scratch, cudaStream_t st) {
     const Dims& d = a.d;
-    a.spec = scratch;
-    a.expt = a.spec + (size_t)a.count * (a.Kcap + kAux) * kSpecStride;
-    a.stash = a.expt + (size_t)a.count * (a.Kcap + kAux) * d.N * d.R * kStates;
+    const ScratchLayout L = scratch_layout(d, a.count, a.Kcap, n_iter, a.nslots, false);
+    a.spec = scratch + L.spec;
+    a.stash = scratch + L.stash;
     const size_t smem = ((kMlpParams * 2 + 15) & ~15) +
                         sizeof(float) * (kGibbsWarps * (kMlpIn + kMlpHid) + a.Kcap) + sizeof(int) * a.Kcap +
                         d.T + 16;
@@ -589,24 +733,28 @@ cudaError_t launch_learned_move(GibbsArgs a, const void* mlp, const float* site_
     return cudaGetLastError();
 }
 
-size_t gibbs_scratch_doubles(const Dims& d, int count, int Kcap) {
-    const size_t spec = (size_t)count * (Kcap + kAux) * kSpecStride;
-    const size_t ex = (size_t)count * (Kcap + kAux) * d.N * d.R * kStates;
-    const size_t stash = (size_t)count * kGibbsWarps * d.NI * kRateBlock * 32;
-    return spec + ex + stash;
+size_t gibbs_scratch_doubles(const Dims& d, int count, int Kcap, int n_iter, int nslots, bool aux) {
+    return scratch_layout(d, count, Kcap, n_iter, nslots, aux).total;
 }
 
 int gibbs_aux() { return kAux; }
 
-cudaError_t launch_gibbs(GibbsArgs a, double* scratch, cudaStream_t st) {
+cudaError_t launch_gibbs(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st) {
     const Dims& d = a.d;
-    a.spec = scratch;
-    a.expt = a.spec + (size_t)a.count * (a.Kcap + kAux) * kSpecStride;
-    a.stash = a.expt + (size_t)a.count * (a.Kcap + kAux) * d.N * d.R * kStates;
-    const size_t smem = sizeof(double) * (size_t)(a.Kcap + kAux) * (d.R + 1) +
+    const ScratchLayout L = scratch_layout(d, a.count, a.Kcap, n_iter, a.nslots, true);
+    a.spec = scratch + L.spec;
+    a.stash = scratch + L.stash;
+    a.aux_ls = scratch + L.aux_ls;
+    a.aux_site = reinterpret_cast<int32_t*>(scratch + L.aux_site);
+    a.aux_rec = scratch + L.aux_rec;
+    a.aux_stash = scratch + L.aux_stash;
+    const size_t tasks = (size_t)a.count * n_iter * kAux;
+    gibbs_aux_kernel<<<aux_grid(tasks), 32 * kAuxWarps, (size_t)kAuxWarps * d.T, st>>>(a, n_iter);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(double) * ((size_t)a.Kcap * d.R + a.Kcap + kAux) +
                         sizeof(int) * (a.Kcap + kAux) + d.T + 16;
-    cudaError_t e = cudaFuncSetAttribute(gibbs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    e = cudaFuncSetAttribute(gibbs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     gibbs_kernel<<<a.count, 32 * kGibbsWarps, smem, st>>>(a);
     return cudaGetLastError();

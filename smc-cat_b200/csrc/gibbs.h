@@ -15,6 +15,15 @@ struct GibbsPart {
     double rates[kMaxRates];
 };
 
+// One internal node of a particle's post-order with the stash slots of its
+// result and of its internal children (-1 for a tip). Slots are handed out
+// from a free list in post-order, so a pass over a tree needs only as many
+// slots as it ever has results waiting for their parent.
+struct GibbsNode {
+    int32_t n, c[2], so;
+    int32_t sc[2], pad[2];
+};
+
 struct GibbsArgs {
     Dims d;
     int count;
@@ -23,7 +32,8 @@ struct GibbsArgs {
     double alpha;           // DPP concentration
     unsigned long long seed;
     const GibbsPart* parts; // [count]
-    const int32_t* tree;    // [count][T-1][3]: internal node, child 1, child 2 in post-order
+    const GibbsNode* nodes; // [count][T-1] in post-order
+    int nslots;             // stash slots a pass needs (maximum over the particles)
     const double* branch;   // [count][2T-1]
     const double* base;     // [count][190]
     double* logits;         // [count][Kcap + aux][20]: in = slots 0..K-1, out = all slots used
@@ -41,20 +51,30 @@ struct GibbsArgs {
     // kernels; those classes then need no single-site pruning per iteration.
     const double* table;
     int Kt;
-    // scratch, set by launch_gibbs
+    // scratch, set by launch_gibbs / launch_learned_move
     double* spec;
-    double* expt;
     double* stash;
+    double* aux_ls;         // [count][n_iter][aux]: site log-likelihood under each auxiliary class
+    int32_t* aux_site;      // [count][n_iter]: the site each iteration draws
+    double* aux_rec;        // spectral records of the auxiliary-class kernel's warps
+    double* aux_stash;      // stash of the auxiliary-class kernel's warps
 };
 
-size_t gibbs_scratch_doubles(const Dims& d, int count, int Kcap);
+// Scratch doubles of one call: `n_iter` site iterations per particle, a
+// post-order needing `nslots` stash slots; `aux` for a Gibbs pass (auxiliary
+// classes evaluated beforehand), not for the learned move.
+size_t gibbs_scratch_doubles(const Dims& d, int count, int Kcap, int n_iter, int nslots, bool aux);
 int gibbs_aux();
-cudaError_t launch_gibbs(GibbsArgs a, double* scratch, cudaStream_t st);
+// A Gibbs pass: the auxiliary-class kernel (every iteration's drawn site and
+// auxiliary classes, all at once), then one sequential CTA per particle.
+cudaError_t launch_gibbs(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st);
 
 // Learned-proposal MH site reassignment: parts[i].n_iter updates per particle
 // among its existing classes, proposals from the scoring MLP (BF16 weights
 // `mlp`, site features [S][21]); accepted / proposed counts per particle.
-cudaError_t launch_learned_move(GibbsArgs a, const void* mlp, const float* site_feat,
+// With a class table (GibbsArgs::table) the two classes' site values are read
+// from it; without one they are pruned per update.
+cudaError_t launch_learned_move(GibbsArgs a, int n_iter, const void* mlp, const float* site_feat,
                                 int32_t* n_acc, int32_t* n_prop, double* scratch, cudaStream_t st);
 
 }  // namespace smccat

@@ -812,7 +812,9 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     const int Kcap = d.Kmax + 64;
     const int ks = Kcap + naux;
     std::vector<GibbsPart> parts(n);
-    std::vector<int32_t> tree((size_t)n * d.NI * 3), assign((size_t)n * d.S);
+    std::vector<GibbsNode> tree((size_t)n * d.NI);
+    std::vector<int32_t> assign((size_t)n * d.S);
+    int nslots = 1;
     std::vector<double> branch((size_t)n * d.N), base((size_t)n * kBase), logits((size_t)n * ks * kStates, 0.0);
     std::vector<double> auxv((size_t)n * naux * kStates, 0.0);
     for (int j = 0; j < n; ++j) {
@@ -825,12 +827,29 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         g.fixed_site = site;
         g.pinv = m.pinv;
         for (int r = 0; r < kMaxRates; ++r) g.rates[r] = m.rates[r];
+        // Stash slots from a free list: a node's result takes a free slot and
+        // its internal children's slots are freed once it has read them.
+        std::vector<int> slot_of_node(d.N, -1), free_slots;
+        int used = 0;
         for (int q = 0; q < d.NI; ++q) {
             const int x = m.post[q];
-            tree[((size_t)j * d.NI + q) * 3 + 0] = x;
-            tree[((size_t)j * d.NI + q) * 3 + 1] = m.kids[2 * x];
-            tree[((size_t)j * d.NI + q) * 3 + 2] = m.kids[2 * x + 1];
+            GibbsNode& g = tree[(size_t)j * d.NI + q];
+            g.n = x;
+            for (int ci = 0; ci < 2; ++ci) {
+                const int ch = m.kids[2 * x + ci];
+                g.c[ci] = ch;
+                g.sc[ci] = ch >= d.T ? slot_of_node[ch] : -1;
+                if (ch >= d.T && slot_of_node[ch] < 0)
+                    return mfail(SMCCAT_ESTATE, "internal post-order lists a parent before its child");
+                if (ch >= d.T) free_slots.push_back(slot_of_node[ch]);
+            }
+            if (free_slots.empty()) free_slots.push_back(used++);
+            g.so = free_slots.back();
+            free_slots.pop_back();
+            g.pad[0] = g.pad[1] = 0;
+            slot_of_node[x] = g.so;
         }
+        nslots = std::max(nslots, used);
         std::copy(m.branch.begin(), m.branch.end(), branch.begin() + (size_t)j * d.N);
         std::copy(m.base.begin(), m.base.end(), base.begin() + (size_t)j * kBase);
         std::copy(m.logits.begin(), m.logits.begin() + (size_t)m.K * kStates,
@@ -843,15 +862,16 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stv);
     // A Gibbs pass evaluates the drawn site under every class at every
-    // iteration. For the classes the particles enter with, those values are
-    // evaluated beforehand for every site in one batched pruning pass per
-    // class (the SIMT pruning kernels' evaluation mode, into the partial
-    // workspaces the committed state does not use) and read from a table.
+    // iteration, the learned move under two. For the classes the particles
+    // enter with, those values are evaluated beforehand for every site in one
+    // batched pruning pass per class (the SIMT pruning kernels' evaluation
+    // mode, into the partial workspaces the committed state does not use) and
+    // read from a table: a pass changes assignments only, never a class.
     const int pfirst = *std::min_element(list.begin(), list.end());
     const int prange = *std::max_element(list.begin(), list.end()) - pfirst + 1;
     DeviceView view;
     bool use_table = false;
-    if (learned_updates == 0 && site < 0 && device_view(c, pfirst, prange, &view) == SMCCAT_OK)
+    if (site < 0 && device_view(c, pfirst, prange, &view) == SMCCAT_OK)
         use_table = view.pa.wt == nullptr && prune_variant_has_eval(d.R, view.fp32, view.variant);
     std::vector<PartHdr> ehdr;
     std::vector<NodeJob> enodes;
@@ -894,10 +914,12 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         }
     }
     // Device buffers for this call (inputs, outputs and kernel scratch).
-    const size_t scratch = gibbs_scratch_doubles(d, n, Kcap);
+    const int n_iter = parts[0].n_iter;
+    if (n_iter >= (1 << 24)) return mfail(SMCCAT_EINVAL, "too many site iterations in one call");
+    const size_t scratch = gibbs_scratch_doubles(d, n, Kcap, n_iter, nslots, learned_updates == 0);
     size_t bytes = 0;
     auto carve = [&](size_t b) { const size_t o = bytes; bytes += (b + 255) & ~size_t(255); return o; };
-    const size_t o_parts = carve(sizeof(GibbsPart) * n), o_tree = carve(tree.size() * 4),
+    const size_t o_parts = carve(sizeof(GibbsPart) * n), o_tree = carve(tree.size() * sizeof(GibbsNode)),
                  o_branch = carve(branch.size() * 8), o_base = carve(base.size() * 8),
                  o_logits = carve(logits.size() * 8), o_assign = carve(assign.size() * 4),
                  o_counts = carve((size_t)n * ks * 4), o_kout = carve((size_t)n * 4),
@@ -924,7 +946,7 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         if (e == cudaSuccess) e = cudaMemcpyAsync(dst, dbuf + o, b, cudaMemcpyDeviceToHost, st);
     };
     up(o_parts, parts.data(), sizeof(GibbsPart) * n);
-    up(o_tree, tree.data(), tree.size() * 4);
+    up(o_tree, tree.data(), tree.size() * sizeof(GibbsNode));
     up(o_branch, branch.data(), branch.size() * 8);
     up(o_base, base.data(), base.size() * 8);
     up(o_logits, logits.data(), logits.size() * 8);
@@ -959,7 +981,8 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         a.alpha = tuning_of(c).t.dpp_alpha;
         a.seed = seed;
         a.parts = reinterpret_cast<const GibbsPart*>(dbuf + o_parts);
-        a.tree = reinterpret_cast<const int32_t*>(dbuf + o_tree);
+        a.nodes = reinterpret_cast<const GibbsNode*>(dbuf + o_tree);
+        a.nslots = nslots;
         a.branch = reinterpret_cast<const double*>(dbuf + o_branch);
         a.base = reinterpret_cast<const double*>(dbuf + o_base);
         a.logits = reinterpret_cast<double*>(dbuf + o_logits);
@@ -975,11 +998,11 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         a.table = use_table ? reinterpret_cast<const double*>(dbuf + o_table) : nullptr;
         a.Kt = d.Kmax;
         if (learned_updates > 0)
-            e = launch_learned_move(a, mlp, site_feat, reinterpret_cast<int32_t*>(dbuf + o_acc),
+            e = launch_learned_move(a, n_iter, mlp, site_feat, reinterpret_cast<int32_t*>(dbuf + o_acc),
                                     reinterpret_cast<int32_t*>(dbuf + o_prop),
                                     reinterpret_cast<double*>(dbuf + o_scr), st);
         else
-            e = launch_gibbs(a, reinterpret_cast<double*>(dbuf + o_scr), st);
+            e = launch_gibbs(a, n_iter, reinterpret_cast<double*>(dbuf + o_scr), st);
     }
     down(assign.data(), o_assign, assign.size() * 4);
     down(counts.data(), o_counts, counts.size() * 4);

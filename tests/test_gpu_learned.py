@@ -120,3 +120,27 @@ def test_learned_move_at_zero_temperature_samples_the_crp_prior():
     stat, pval = stats.chisquare(obs, p * obs.sum())
     assert pval > 1e-3, (pval, obs.tolist(), (p * obs.sum()).tolist())
     eng.close()
+
+
+def test_learned_move_table_matches_per_update_pruning():
+    """The learned move reads its two classes' site log-likelihoods from the
+    class table the SIMT pruning kernels fill before the pass; with a kernel
+    variant that has no evaluation mode (the FP64 tensor-path kernels) it
+    prunes the site under both classes at every update instead. Same state,
+    network and seed: the same proposals and decisions, hence the same
+    assignments."""
+    out = []
+    for variant in (None, "dmma"):
+        eng, codes, cfg = cat_engine(seed=33, n=6)
+        eng.learned_params(set_to=(np.random.default_rng(5).normal(size=smccat.MLP_PARAMS) * 0.1)
+                           .astype(np.float32))
+        if variant == "dmma":
+            n, _ = eng.kernel_variants()
+            eng.set_kernel_variant(n - 1)
+        r = eng.learned_move(updates=300, temperature=1.0, seed=9)
+        out.append((eng.get_particles()["assign"], r["accepted"], r["proposed"], eng.lnl()))
+        eng.close()
+    (a, acc_a, prop_a, la), (b, acc_b, prop_b, lb) = out
+    assert prop_a == prop_b and acc_a == acc_b
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_allclose(la, lb, rtol=1e-9)
