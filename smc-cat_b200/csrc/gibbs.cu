@@ -341,22 +341,32 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
     const double* auxl = a.aux_ls + (size_t)i * gp.n_iter * kAux;
     const int32_t* auxs = a.aux_site + (size_t)i * gp.n_iter;
 
-    if (threadIdx.x == 0) s_kcur = gp.K;
+    // Table mode resumes where the particle's last round stopped.
+    const bool tabmode = a.table != nullptr;
+    const int it0 = tabmode ? a.resume_it[i] : 0;
+    const int kstart = tabmode ? a.resume_kcur[i] : gp.K;
+    if (it0 >= gp.n_iter) return;  // finished in an earlier round (uniform)
+    if (threadIdx.x == 0) s_kcur = kstart;
     for (int k = threadIdx.x; k < Kcap + kAux; k += blockDim.x) counts[k] = 0;
     __syncthreads();
     for (int x = threadIdx.x; x < d.S; x += blockDim.x) atomicAdd(&counts[assign[x]], 1);
-    // Classes [0, K0) read their site log-likelihoods from the table; the
-    // others (all of them without a table) are pruned per site below.
-    const int K0 = a.table ? gp.K : 0;
-    const double* tab = a.table ? a.table + (size_t)i * a.Kt * d.S : nullptr;
-    if (warp < kAux)  // one shared workspace per decomposing warp
-        for (int k = K0 + warp; k < gp.K; k += kAux)
+    // Classes [0, K0) read their site log-likelihoods from the table: the entry
+    // classes and those opened in earlier rounds (whose columns the caller has
+    // filled). The others are pruned per site below: in table mode the classes
+    // opened into slots at or above Kt (diagonalised when they opened),
+    // without a table every class.
+    const int K0 = tabmode ? min(kstart, a.Kt) : 0;
+    const double* tab = tabmode ? a.table + (size_t)i * a.Kt * d.S : nullptr;
+    if (!tabmode && warp < kAux)  // one shared workspace per decomposing warp
+        for (int k = warp; k < gp.K; k += kAux)
             spectral_decompose_warp_ws(base, logits + (size_t)k * kStates,
                                        spec + (size_t)k * kSpecStride, work[warp]);
     __syncthreads();
 
     const double alpha_split = log(a.alpha / kAux);
-    for (int it = 0; it < gp.n_iter; ++it) {
+    int stop = gp.n_iter;  // table mode: the iteration after a birth into a table slot
+    bool stopped = false;
+    for (int it = it0; it < gp.n_iter; ++it) {
         // 1. the drawn site leaves its class (Particle.cpp:808-821)
         if (threadIdx.x == 0) {
             const int s = auxs[it];
@@ -436,23 +446,44 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
         const int choice = s_choice;
         if (choice < 0) break;  // weights mode: nothing changes
         if (choice >= kcur) {
-            // The drawn auxiliary becomes class slot kcur.
+            // The drawn auxiliary becomes class slot kcur. In table mode a slot
+            // below Kt gets a table column: its spectral record also goes to the
+            // engine's workspace and the round ends here.
+            const bool to_table = tabmode && kcur < a.Kt;
             if (warp == 0) {
                 if (lane == 0) draw_aux_logits(a.seed, gp.p, it, choice - kcur, logits + (size_t)kcur * kStates);
                 __syncwarp();
-                spectral_decompose_warp_ws(base, logits + (size_t)kcur * kStates,
-                                           spec + (size_t)kcur * kSpecStride, work[0]);
+                double* rec = spec + (size_t)kcur * kSpecStride;
+                spectral_decompose_warp_ws(base, logits + (size_t)kcur * kStates, rec, work[0]);
+                __syncwarp();
+                if (to_table) {
+                    const size_t ek = (size_t)gp.p * d.Kmax + kcur;
+                    double* er = a.eng_spec + (ek * 2 + (a.eng_sws[ek] & kSwsSpec)) * kSpecStride;
+                    for (int x = lane; x < kSpecStride; x += 32) er[x] = rec[x];
+                }
                 if (lane == 0) {
                     assign[s] = kcur;
                     counts[kcur] = 1;
                     s_kcur = kcur + 1;
                 }
             }
+            if (to_table) {
+                stop = it + 1;
+                stopped = true;
+                break;  // uniform: every thread saw the same choice and slot
+            }
         } else if (threadIdx.x == 0) {
             assign[s] = choice;
             counts[choice]++;
         }
         __syncthreads();
+    }
+    __syncthreads();
+    if (tabmode && threadIdx.x == 0) {
+        a.resume_it[i] = stop;
+        a.resume_kcur[i] = s_kcur;
+        // The new class's column is needed only if iterations remain.
+        a.born[i] = (stopped && stop < gp.n_iter) ? s_kcur - 1 : -1;
     }
     for (int k = threadIdx.x; k < s_kcur; k += blockDim.x) a.counts[(size_t)i * (Kcap + kAux) + k] = counts[k];
     if (threadIdx.x == 0) a.kout[i] = s_kcur;
@@ -730,6 +761,21 @@ cudaError_t launch_learned_move(GibbsArgs a, int n_iter, const void* mlp, const 
     if (e != cudaSuccess) return e;
     learned_move_kernel<<<a.count, 32 * kGibbsWarps, smem, st>>>(
         a, static_cast<const __nv_bfloat16*>(mlp), site_feat, n_acc, n_prop);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gibbs_resume(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st) {
+    const Dims& d = a.d;
+    const ScratchLayout L = scratch_layout(d, a.count, a.Kcap, n_iter, a.nslots, true);
+    a.spec = scratch + L.spec;
+    a.stash = scratch + L.stash;
+    a.aux_ls = scratch + L.aux_ls;
+    a.aux_site = reinterpret_cast<int32_t*>(scratch + L.aux_site);
+    a.aux_rec = scratch + L.aux_rec;
+    a.aux_stash = scratch + L.aux_stash;
+    const size_t smem = sizeof(double) * ((size_t)a.Kcap * d.R + a.Kcap + kAux) +
+                        sizeof(int) * (a.Kcap + kAux) + d.T + 16;
+    gibbs_kernel<<<a.count, 32 * kGibbsWarps, smem, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -51,6 +51,17 @@ struct GibbsArgs {
     // kernels; those classes then need no single-site pruning per iteration.
     const double* table;
     int Kt;
+    // Table mode: a pass runs in rounds. A particle stops at a birth into a
+    // slot below Kt, with the new class's spectral record written to the
+    // engine's spectral workspace (eng_spec, half from eng_sws) and the slot in
+    // born[i]; the caller evaluates that class's table column with the pruning
+    // kernels and relaunches, and the particle resumes at resume_it[i] with
+    // resume_kcur[i] slots. born[i] = -1 once the particle has finished.
+    int32_t* resume_it;
+    int32_t* resume_kcur;
+    int32_t* born;
+    double* eng_spec;
+    const uint8_t* eng_sws;
     // scratch, set by launch_gibbs / launch_learned_move
     double* spec;
     double* stash;
@@ -68,6 +79,8 @@ int gibbs_aux();
 // A Gibbs pass: the auxiliary-class kernel (every iteration's drawn site and
 // auxiliary classes, all at once), then one sequential CTA per particle.
 cudaError_t launch_gibbs(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st);
+// The next round of a table-mode pass (the sequential kernel alone).
+cudaError_t launch_gibbs_resume(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st);
 
 // Learned-proposal MH site reassignment: parts[i].n_iter updates per particle
 // among its existing classes, proposals from the scoring MLP (BF16 weights

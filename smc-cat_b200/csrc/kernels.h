@@ -62,6 +62,10 @@ struct PruneArgs {
     int eval_k = -1;
     const int32_t* eval_map = nullptr;
     double* eval_out = nullptr;
+    // Per-particle evaluation: when set, particle p is evaluated under class
+    // eval_kp[p - first] (any slot below Kmax whose matrices and spectral
+    // record are in place; -1 skips the particle) and eval_k is not used.
+    const int32_t* eval_kp = nullptr;
 };
 
 cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d, cudaStream_t st);

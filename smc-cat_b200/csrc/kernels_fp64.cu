@@ -322,7 +322,7 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     double* LSCp = a.LSC + (size_t)p * d.NI * 2 * lws_stride;
     // The class whose matrices and frequencies the tile runs: its own, or the
     // class under evaluation.
-    const int ek = a.eval_k;
+    const int ek = a.eval_kp ? a.eval_kp[p - a.first] : a.eval_k;
     const int kc = ek >= 0 ? ek : tl.k;
     const T* Pcls = static_cast<const T*>(a.Pm) +
                     ((size_t)p * d.Kmax + kc) * d.N * 2 * (size_t)R * kPBlock + (size_t)r * kPBlock;
@@ -339,7 +339,8 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     __syncthreads();
     if (!h->active) return true;  // uniform across the CTA (after the barriers exist)
     const int ej = ek >= 0 ? a.eval_map[p - a.first] : 0;
-    if (ek >= 0 && (ej < 0 || ek >= h->num_classes)) return true;  // uniform as well
+    if (a.eval_kp ? (ek < 0 || ej < 0) : (ek >= 0 && (ej < 0 || ek >= h->num_classes)))
+        return true;  // uniform as well
 
     // A class-local refresh of another class leaves this tile's partials as
     // they are: only its root reduction reruns. In evaluation mode the plan

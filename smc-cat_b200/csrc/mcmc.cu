@@ -927,11 +927,35 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
                  o_status = carve(4), o_scr = carve(scratch * 8), o_acc = carve((size_t)n * 4),
                  o_prop = carve((size_t)n * 4);
     size_t o_ehdr = 0, o_enodes = 0, o_emap = 0, o_table = 0;
+    // A table-mode Gibbs pass runs in rounds (classes opened into table slots
+    // get their columns between rounds): per-particle resume state, the
+    // transition-matrix jobs of every particle's branches and the per-round
+    // evaluation classes.
+    const bool rounds = use_table && learned_updates == 0;
+    const int nbr = d.N - 1, nchunk = (nbr + kPmChunk - 1) / kPmChunk;
+    size_t o_rit = 0, o_rk = 0, o_born = 0, o_pjobs = 0, o_pmjobs = 0, o_ekp = 0;
+    std::vector<int32_t> rit(n, 0), rk(n), born(n, -1);
+    std::vector<PJob> pjobs;
     if (use_table) {
         o_ehdr = carve(sizeof(PartHdr) * ehdr.size());
         o_enodes = carve(sizeof(NodeJob) * enodes.size());
         o_emap = carve(4 * emap.size());
         o_table = carve((size_t)n * d.Kmax * d.S * 8);
+    }
+    if (rounds) {
+        o_rit = carve((size_t)n * 4);
+        o_rk = carve((size_t)n * 4);
+        o_born = carve((size_t)n * 4);
+        o_pjobs = carve(sizeof(PJob) * (size_t)n * nbr);
+        o_pmjobs = carve(sizeof(PmJob) * (size_t)n * nchunk);
+        o_ekp = carve((size_t)prange * 4);
+        pjobs.reserve((size_t)n * nbr);
+        for (int j = 0; j < n; ++j) {
+            const Mirror& m = slot_of(c, list[j]).cur;
+            rk[j] = m.K;
+            for (int x = 0; x < d.N; ++x)
+                if (x != m.root) pjobs.push_back(PJob{list[j], x, m.pws[x], 0, m.branch[x]});
+        }
     }
     char* dbuf = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&dbuf, bytes, st);
@@ -953,6 +977,13 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     up(o_assign, assign.data(), assign.size() * 4);
     up(o_aux, auxv.data(), auxv.size() * 8);
     if (e == cudaSuccess) e = cudaMemsetAsync(dbuf + o_status, 0, 4, st);
+    if (rounds) {
+        up(o_rit, rit.data(), (size_t)n * 4);
+        up(o_rk, rk.data(), (size_t)n * 4);
+        up(o_born, born.data(), (size_t)n * 4);
+        up(o_pjobs, pjobs.data(), sizeof(PJob) * pjobs.size());
+    }
+    PruneArgs pa{};
     if (use_table) {
         up(o_ehdr, ehdr.data(), sizeof(PartHdr) * ehdr.size());
         up(o_enodes, enodes.data(), sizeof(NodeJob) * enodes.size());
@@ -962,7 +993,7 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(const_cast<uint8_t*>(view.sws) + (size_t)pfirst * d.Kmax, esws.data(),
                                 esws.size(), cudaMemcpyHostToDevice, st);
-        PruneArgs pa = view.pa;
+        pa = view.pa;
         pa.hdr = reinterpret_cast<const PartHdr*>(dbuf + o_ehdr);
         pa.nodes = reinterpret_cast<const NodeJob*>(dbuf + o_enodes);
         pa.eval_map = reinterpret_cast<const int32_t*>(dbuf + o_emap);
@@ -997,12 +1028,51 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         a.status = reinterpret_cast<int*>(dbuf + o_status);
         a.table = use_table ? reinterpret_cast<const double*>(dbuf + o_table) : nullptr;
         a.Kt = d.Kmax;
+        double* scr = reinterpret_cast<double*>(dbuf + o_scr);
+        if (rounds) {
+            a.resume_it = reinterpret_cast<int32_t*>(dbuf + o_rit);
+            a.resume_kcur = reinterpret_cast<int32_t*>(dbuf + o_rk);
+            a.born = reinterpret_cast<int32_t*>(dbuf + o_born);
+            a.eng_spec = const_cast<double*>(view.spec);
+            a.eng_sws = view.sws;
+        }
         if (learned_updates > 0)
             e = launch_learned_move(a, n_iter, mlp, site_feat, reinterpret_cast<int32_t*>(dbuf + o_acc),
-                                    reinterpret_cast<int32_t*>(dbuf + o_prop),
-                                    reinterpret_cast<double*>(dbuf + o_scr), st);
+                                    reinterpret_cast<int32_t*>(dbuf + o_prop), scr, st);
         else
-            e = launch_gibbs(a, n_iter, reinterpret_cast<double*>(dbuf + o_scr), st);
+            e = launch_gibbs(a, n_iter, scr, st);
+        // Rounds: the classes the last round opened into table slots get
+        // their transition matrices and table columns (the pruning kernels'
+        // evaluation mode, one class per particle), then the particles resume.
+        // Each round opens at least one class, so there are at most Kmax.
+        std::vector<int32_t> ekp(prange);
+        std::vector<PmJob> mj;
+        PruneArgs pb = pa;
+        pb.eval_k = -1;
+        pb.eval_kp = reinterpret_cast<const int32_t*>(dbuf + o_ekp);
+        for (int round = 0; rounds && round <= d.Kmax && e == cudaSuccess; ++round) {
+            down(born.data(), o_born, (size_t)n * 4);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) break;
+            mj.clear();
+            std::fill(ekp.begin(), ekp.end(), -1);
+            for (int j = 0; j < n; ++j) {
+                if (born[j] < 0) continue;
+                const int q = list[j] - pfirst;
+                ekp[q] = born[j];
+                for (int c0 = 0; c0 < nbr; c0 += kPmChunk)
+                    mj.push_back(PmJob{q, born[j], j * nbr + c0, std::min(kPmChunk, nbr - c0)});
+            }
+            if (mj.empty()) break;
+            up(o_pmjobs, mj.data(), sizeof(PmJob) * mj.size());
+            up(o_ekp, ekp.data(), (size_t)prange * 4);
+            if (e == cudaSuccess)
+                e = launch_pmat(reinterpret_cast<const PmJob*>(dbuf + o_pmjobs), (int)mj.size(),
+                                reinterpret_cast<const PJob*>(dbuf + o_pjobs), pa.hdr, pfirst, view.sws,
+                                view.spec, view.Pm, view.fp32, d, st);
+            if (e == cudaSuccess) e = launch_prune(pb, view.ntiles, view.variant, st);
+            if (e == cudaSuccess) e = launch_gibbs_resume(a, n_iter, scr, st);
+        }
     }
     down(assign.data(), o_assign, assign.size() * 4);
     down(counts.data(), o_counts, counts.size() * 4);
