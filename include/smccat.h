@@ -432,14 +432,19 @@ typedef struct smccat_learned_stats {
 
 /* Metropolis-Hastings class reassignment with the learned proposal for the
  * masked particles of [first, first+count): `updates` random-site updates per
- * particle; each proposes a class from the softmax of the MLP scores (BF16
- * weights, FP32 arithmetic) among the existing classes and accepts with the
- * tempered likelihood ratio, the CRP prior ratio n_b / (n_a - 1) and the
- * proposal ratio, so the posterior is unchanged. Sites whose class would empty
- * are not moved. Then refreshLikelihood(true). */
+ * particle; each proposes a class from the softmax of the MLP scores among the
+ * existing classes and accepts with the tempered likelihood ratio, the CRP
+ * prior ratio n_b / (n_a - 1) and the proposal ratio, so the posterior is
+ * unchanged. Sites whose class would empty are not moved. Then
+ * refreshLikelihood(true). The scores run on the tensor cores: BF16 weights,
+ * feature rows and hidden activations, FP32 accumulation. */
 int smccat_learned_move(smccat_ctx* ctx, int32_t first, int32_t count, const uint8_t* mask,
                         int32_t updates, double temperature, uint64_t seed,
                         smccat_learned_stats* stats);
+
+/* The learned proposal's scores of every class of particle p at `site` (the
+ * values smccat_learned_move draws from), into out[num_classes of p]. */
+int smccat_learned_scores(smccat_ctx* ctx, int32_t p, int32_t site, double* out);
 
 /* computeNextStep (Miscellaneous.hpp:42-109) in FP64 on the device, on the
  * current log-likelihoods of [first, first+count): bisects the temperature

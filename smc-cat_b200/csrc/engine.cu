@@ -893,6 +893,7 @@ int smccat::refresh_internal(smccat_ctx* c, int first, int count, int mode, cons
 }
 
 const Slot& smccat::slot_of(const smccat_ctx* c, int p) { return c->slots[p]; }
+int smccat::particles_of(const smccat_ctx* c) { return (int)c->slots.size(); }
 Slot& smccat::slot_mut(smccat_ctx* c, int p) { return c->slots[p]; }
 bool smccat::rebuild_tree(int T, const int32_t* parent, Mirror* m) { return build_tree(T, parent, m); }
 
@@ -947,6 +948,7 @@ int smccat::device_view(smccat_ctx* c, int first, int count, DeviceView* v) {
 }
 const Dims& smccat::dims_of(const smccat_ctx* c) { return c->d; }
 int smccat::model_flags_of(const smccat_ctx* c) { return c->cfg.model_flags; }
+uint32_t smccat::wait_limit_of(const smccat_ctx* c) { return c->wait_limit; }
 const double* smccat::lnl_device(const smccat_ctx* c) { return c->d_lnl; }
 const uint8_t* smccat::codes_device(const smccat_ctx* c) { return c->d_codes; }
 const uint8_t* smccat::codes_host(const smccat_ctx* c) { return c->codes.data(); }

@@ -67,8 +67,10 @@ int refresh_internal(smccat_ctx* c, int first, int count, int mode, const uint8_
 
 // Host mirror of one slot (read-only view for the MCMC driver).
 const Slot& slot_of(const smccat_ctx* c, int p);
+int particles_of(const smccat_ctx* c);  // particle slots of the context
 const Dims& dims_of(const smccat_ctx* c);
 int model_flags_of(const smccat_ctx* c);
+uint32_t wait_limit_of(const smccat_ctx* c);  // polls per bounded device wait
 const double* lnl_device(const smccat_ctx* c);  // [max_particles] current log-likelihoods
 const uint8_t* codes_device(const smccat_ctx* c);   // [T][S]
 const double* isinv_device(const smccat_ctx* c);    // [S]

@@ -101,9 +101,8 @@ __device__ __forceinline__ double warp_incl_scan(double x) {
 }
 
 // Rates per warp in the Gibbs weights (all of a class's rates together) and in
-// the learned move (which spreads its two classes' rates over more warps).
+// the learned move.
 constexpr int kRateBlock = 4;
-constexpr int kRateBlockLearned = 2;
 
 // Log-likelihoods of one site under one class for rates [r0, r0 + RB) (those
 // below R), one warp: lanes are states and the rate chains interleave.
@@ -491,121 +490,330 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
 
 // ---------------------------------------------------------------------------
 // Learned-proposal site reassignment.
+//
+// One CTA of 128 threads per particle. The scoring MLP runs on the
+// 5th-generation tensor cores: the feature rows of up to 128 classes are one
+// M = 128 operand in tensor memory (thread t writes row t, BF16), each layer
+// is one tcgen05.mma kind::f16 product against the BF16 weights, staged once
+// in shared memory in the K-major canonical layout (no swizzle), with FP32
+// accumulation in tensor memory; thread t reads its row back for the bias,
+// the ReLU and the next layer's operand (or the final dot product):
+//   layer 1: D[c][j] = sum_i X[c][i] W1[i][j]   M = 128, N = 128, K = 48 (44 inputs)
+//   layer 2: D[c][j] = sum_i H[c][i] W2[i][j]   M = 128, N = 128, K = 128
+// Tensor-memory columns: X [0, 24), D [32, 160), H [160, 224).
+// A class's score depends on its own row only, so the reverse scores (two
+// classes with updated sizes) come from the same products as the forward ones.
+constexpr int kLmThreads = 128;
+constexpr int kLmK1 = 48;
+constexpr uint32_t kLmCols = 256;
+constexpr uint32_t kLmColX = 0, kLmColD = 32, kLmColH = 160;
+constexpr uint32_t kLmLbo = 128;                   // next core matrix along K
+constexpr uint32_t kLmSbo1 = (kLmK1 / 8) * 128;    // W1: next 8-row group
+constexpr uint32_t kLmSbo2 = (kMlpHid / 8) * 128;  // W2: next 8-row group
+constexpr uint32_t kLmW1Bytes = kMlpHid * kLmK1 * 2;
+constexpr uint32_t kLmW2Bytes = kMlpHid * kMlpHid * 2;
+// idesc: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), K-major A
+// and B, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t kLmIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kMlpHid >> 3) << 17) |
+                              ((uint32_t)(kLmThreads >> 4) << 24);
 
-// Score of one (site, class) feature row x (kMlpIn floats, shared) by one warp;
-// W is the BF16 parameter vector in shared memory, h a 128-float warp buffer.
-__device__ float mlp_score(const __nv_bfloat16* W, const float* x, float* h) {
-    const int lane = threadIdx.x & 31;
-    float h1[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int j = lane + 32 * q;
-        float v = __bfloat162float(W[kMlpB1 + j]);
-        for (int i = 0; i < kMlpIn; ++i) v = fmaf(x[i], __bfloat162float(W[kMlpW1 + i * kMlpHid + j]), v);
-        h1[q] = fmaxf(v, 0.f);
-    }
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < 4; ++q) h[lane + 32 * q] = h1[q];
-    __syncwarp();
-    float part = 0.f;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int j = lane + 32 * q;
-        float v = __bfloat162float(W[kMlpB2 + j]);
-        for (int i = 0; i < kMlpHid; ++i) v = fmaf(h[i], __bfloat162float(W[kMlpW2 + i * kMlpHid + j]), v);
-        part = fmaf(fmaxf(v, 0.f), __bfloat162float(W[kMlpW3 + j]), part);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-    return part + __bfloat162float(W[kMlpB3]);
+__device__ __forceinline__ uint32_t lm_sa(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Feature row of (site features sf, class stationary pi, class size n) by one warp.
-__device__ void mlp_features(const float* sf, const double* pi, int n, float* x) {
-    const int lane = threadIdx.x & 31;
-    if (lane < kSiteFeat) x[lane] = sf[lane];
-    if (lane < kStates) x[kSiteFeat + lane] = (float)pi[lane];
-    double dot = (lane < kStates) ? sf[lane] * log(pi[lane]) : 0.0;
-    dot = wsum(dot);
-    if (lane == 0) {
+// Byte offset of element (n, k) of a K-major canonical BF16 tile (8-row x
+// 16-byte core matrices).
+__device__ __forceinline__ uint32_t lm_kmaj(int n, int k, uint32_t sbo) {
+    return (n >> 3) * sbo + (k >> 3) * kLmLbo + (n & 7) * 16 + (k & 7) * 2;
+}
+
+__device__ __forceinline__ uint64_t lm_desc(uint32_t addr, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)(kLmLbo >> 4) << 16) |
+           ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void lm_st8(uint32_t taddr, const uint32_t* v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+                 : "memory");
+}
+
+__device__ __forceinline__ void lm_ld8(uint32_t taddr, uint32_t* v) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                   "=r"(v[7])
+                 : "r"(taddr)
+                 : "memory");
+}
+
+__device__ __forceinline__ void lm_mma(uint32_t d, uint32_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %3, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %4, p;\n\t}" ::"r"(d),
+        "r"(a), "l"(b), "r"(acc), "r"(kLmIdesc)
+        : "memory");
+}
+
+__device__ __forceinline__ void lm_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(lm_sa(bar))
+                 : "memory");
+}
+
+__device__ __noinline__ bool lm_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(lm_sa(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const uint32_t l = __bfloat16_as_ushort(__float2bfloat16_rn(lo));
+    const uint32_t h = __bfloat16_as_ushort(__float2bfloat16_rn(hi));
+    return l | (h << 16);
+}
+
+// Shared state of the learned-move CTA's tensor-core scoring.
+struct LmState {
+    uint32_t tm;       // tensor-memory base
+    uint64_t* bar;     // product-completion barrier
+    uint32_t phase;    // its next parity
+    bool pend;         // thread 0: a committed product not yet waited on
+    uint32_t limit;
+};
+
+// One product of the CTA (thread 0 issues, every thread waits for it).
+// `ok` is uniform on entry and on return.
+__device__ bool lm_product(LmState& s, bool ok, uint32_t acol, uint32_t bbase, uint32_t sbo, int ksteps,
+                           int* status) {
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    ok = __syncthreads_and(ok);
+    if (!ok) return false;
+    if (threadIdx.x == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        for (int ks = 0; ks < ksteps; ++ks)
+            lm_mma(s.tm + kLmColD, s.tm + acol + 8 * ks, lm_desc(bbase + ks * 2 * kLmLbo, sbo), ks > 0);
+        lm_commit(s.bar);
+        s.pend = true;
+    }
+    bool got = lm_wait(s.bar, s.phase, s.limit);
+    if (got) {
+        s.phase ^= 1u;
+        if (threadIdx.x == 0) s.pend = false;
+    } else {
+        atomicOr(status, 8);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return __syncthreads_and(got);
+}
+
+// Scores of the feature rows each thread has just written to columns
+// [kLmColX, +24) of its lane: both layers and the final dot product. Thread t
+// gets its own row's score.
+__device__ bool lm_scores(LmState& s, bool ok, const unsigned char* w1t, const unsigned char* w2t,
+                          const float* b1, const float* b2, const float* w3, float b3, int* status,
+                          float* out) {
+    const uint32_t tl = s.tm + ((uint32_t)((threadIdx.x >> 5) * 32) << 16);  // this warp's lane quarter
+    ok = lm_product(s, ok, kLmColX, lm_sa(w1t), kLmSbo1, kLmK1 / 16, status);
+    if (ok) {
+        for (int c16 = 0; c16 < kMlpHid / 16; ++c16) {
+            uint32_t v[16], h[8];
+            lm_ld8(tl + kLmColD + 16 * c16, v);
+            lm_ld8(tl + kLmColD + 16 * c16 + 8, v + 8);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int j = 16 * c16 + 2 * q;
+                h[q] = pack_bf16(fmaxf(__uint_as_float(v[2 * q]) + b1[j], 0.f),
+                                 fmaxf(__uint_as_float(v[2 * q + 1]) + b1[j + 1], 0.f));
+            }
+            lm_st8(tl + kLmColH + 8 * c16, h);
+        }
+    }
+    ok = lm_product(s, ok, kLmColH, lm_sa(w2t), kLmSbo2, kMlpHid / 16, status);
+    float sc = b3;
+    if (ok) {
+        for (int c16 = 0; c16 < kMlpHid / 16; ++c16) {
+            uint32_t v[16];
+            lm_ld8(tl + kLmColD + 16 * c16, v);
+            lm_ld8(tl + kLmColD + 16 * c16 + 8, v + 8);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int j = 16 * c16 + q;
+                sc = fmaf(fmaxf(__uint_as_float(v[q]) + b2[j], 0.f), w3[j], sc);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    *out = sc;
+    return ok;
+}
+
+// This thread's feature row (site features sf, class stationary pi and its
+// logarithm, class size n) into tensor-memory columns [kLmColX, +24) of its lane;
+// zeros for a row without a class.
+__device__ void lm_features(uint32_t tl, const float* sf, const float* pi, const float* lpi, int n, bool on) {
+    float x[kLmK1];
+#pragma unroll
+    for (int i = 0; i < kLmK1; ++i) x[i] = 0.f;
+    if (on) {
+        float dot = 0.f;
+#pragma unroll
+        for (int i = 0; i < kSiteFeat; ++i) x[i] = sf[i];
+#pragma unroll
+        for (int m = 0; m < kStates; ++m) {
+            x[kSiteFeat + m] = pi[m];
+            dot = fmaf(sf[m], lpi[m], dot);
+        }
         x[kSiteFeat + 20] = logf((float)(n > 1 ? n : 1));
-        x[kSiteFeat + 21] = (float)dot;
-        x[kSiteFeat + 22] = 0.f;
+        x[kSiteFeat + 21] = dot;
     }
-    __syncwarp();
+    uint32_t u[kLmK1 / 2];
+#pragma unroll
+    for (int q = 0; q < kLmK1 / 2; ++q) u[q] = pack_bf16(x[2 * q], x[2 * q + 1]);
+#pragma unroll
+    for (int c8 = 0; c8 < kLmK1 / 16; ++c8) lm_st8(tl + kLmColX + 8 * c8, u + 8 * c8);
 }
 
-__global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArgs a,
-                                                                        const __nv_bfloat16* mlp,
-                                                                        const float* site_feat,
-                                                                        int32_t* n_acc, int32_t* n_prop) {
+__global__ void __launch_bounds__(kLmThreads) learned_move_kernel(GibbsArgs a, const __nv_bfloat16* mlp,
+                                                                  const float* site_feat, int32_t* n_acc,
+                                                                  int32_t* n_prop) {
     const Dims& d = a.d;
     const int i = blockIdx.x;
     const GibbsPart gp = a.parts[i];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int K = gp.K;
     double* spec = a.spec + (size_t)i * a.Kcap * kSpecStride;
-    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * a.nslots * kRateBlockLearned * 32;
+    double* stash = a.stash + ((size_t)i * kGibbsWarps + warp) * a.nslots * kRateBlock * 32;
     // With the class table the two classes' site values are looked up;
     // without it they are pruned per update.
     const bool tabled = a.table != nullptr;
     const double* tab = tabled ? a.table + (size_t)i * a.Kt * d.S : nullptr;
-    __shared__ __align__(16) double xch[kGibbsWarps][kRateBlockLearned * kStates];
+    __shared__ __align__(16) double xch[kLmThreads / 32][kRateBlock * kStates];
     const double* logits = a.logits + (size_t)i * (a.Kcap + kAux) * kStates;
     int32_t* assign = a.assign + (size_t)i * d.S;
     const double* base = a.base + (size_t)i * kBase;
-    extern __shared__ __align__(16) unsigned char lsm[];
-    __nv_bfloat16* W = reinterpret_cast<__nv_bfloat16*>(lsm);              // kMlpParams
-    float* xs = reinterpret_cast<float*>(lsm + ((kMlpParams * 2 + 15) & ~15));  // [warps][kMlpIn]
-    float* hs = xs + kGibbsWarps * kMlpIn;                                   // [warps][kMlpHid]
-    float* score = hs + kGibbsWarps * kMlpHid;                               // [Kcap]
-    int* counts = reinterpret_cast<int*>(score + a.Kcap);                   // [Kcap]
-    uint8_t* scode = reinterpret_cast<uint8_t*>(counts + a.Kcap);           // [T]
+    extern __shared__ __align__(1024) unsigned char lsm[];
+    unsigned char* w1t = lsm;                                  // W1 tile
+    unsigned char* w2t = lsm + kLmW1Bytes;                     // W2 tile
+    float* bias = reinterpret_cast<float*>(w2t + kLmW2Bytes);  // b1, b2, w3 [3][kMlpHid]
+    float* pis = bias + 3 * kMlpHid;                           // [Kcap][20]
+    float* lpis = pis + (size_t)a.Kcap * kStates;              // [Kcap][20]
+    float* score = lpis + (size_t)a.Kcap * kStates;            // [Kcap]
+    int* counts = reinterpret_cast<int*>(score + a.Kcap);      // [Kcap]
+    uint8_t* scode = reinterpret_cast<uint8_t*>(counts + a.Kcap);  // [T]
     __shared__ double lrate[2][kMaxRates];
-    __shared__ float rev[2];
+    __shared__ float rev[2], sfs[kSiteFeat];
     __shared__ int s_site, s_a, s_b;
     __shared__ curandStatePhilox4_32_10_t rng_state;
-    __shared__ SpecWork work[kAux];
+    __shared__ SpecWork work[kLmThreads / 32];
     __shared__ int acc_n, prop_n;
+    __shared__ __align__(8) uint64_t mma_bar;
+    __shared__ uint32_t tmem_slot;
 
-    for (int x = threadIdx.x; x < kMlpParams; x += blockDim.x) W[x] = mlp[x];
-    for (int k = threadIdx.x; k < a.Kcap; k += blockDim.x) counts[k] = 0;
-    if (threadIdx.x == 0) {
+    // Weights: the two layer tiles in the canonical layout, biases and the
+    // output row in FP32.
+    for (int x = tid; x < kMlpHid * kLmK1; x += kLmThreads) {
+        const int n = x / kLmK1, k = x % kLmK1;
+        const __nv_bfloat16 w = k < kMlpIn ? mlp[kMlpW1 + k * kMlpHid + n] : __float2bfloat16_rn(0.f);
+        *reinterpret_cast<__nv_bfloat16*>(w1t + lm_kmaj(n, k, kLmSbo1)) = w;
+    }
+    for (int x = tid; x < kMlpHid * kMlpHid; x += kLmThreads) {
+        const int n = x / kMlpHid, k = x % kMlpHid;
+        *reinterpret_cast<__nv_bfloat16*>(w2t + lm_kmaj(n, k, kLmSbo2)) = mlp[kMlpW2 + k * kMlpHid + n];
+    }
+    for (int j = tid; j < kMlpHid; j += kLmThreads) {
+        bias[j] = __bfloat162float(mlp[kMlpB1 + j]);
+        bias[kMlpHid + j] = __bfloat162float(mlp[kMlpB2 + j]);
+        bias[2 * kMlpHid + j] = __bfloat162float(mlp[kMlpW3 + j]);
+    }
+    const float b3 = __bfloat162float(mlp[kMlpB3]);
+    // Class stationary distributions (softmax of the logits) and their logs.
+    for (int k = tid; k < K; k += kLmThreads) {
+        const double* lg = logits + (size_t)k * kStates;
+        double e[kStates], tot = 0.0;
+        for (int m = 0; m < kStates; ++m) { e[m] = exp(lg[m]); tot += e[m]; }
+        for (int m = 0; m < kStates; ++m) {
+            const double pv = e[m] / tot;
+            pis[(size_t)k * kStates + m] = (float)pv;
+            lpis[(size_t)k * kStates + m] = (float)log(pv);
+        }
+    }
+    for (int k = tid; k < a.Kcap; k += kLmThreads) counts[k] = 0;
+    if (tid == 0) {
         curand_init(a.seed, (unsigned long long)gp.p, 0ull, &rng_state);
         acc_n = prop_n = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(lm_sa(&mma_bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(lm_sa(&tmem_slot)),
+                     "r"(kLmCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    // The weight tiles are read by the tensor cores (the async proxy).
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    for (int x = threadIdx.x; x < d.S; x += blockDim.x) atomicAdd(&counts[assign[x]], 1);
-    if (warp < kAux)
-        for (int k = warp; k < K; k += kAux)
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    LmState ls{tmem_slot, &mma_bar, 0u, false, a.wait_limit};
+    const uint32_t tl = ls.tm + ((uint32_t)(warp * 32) << 16);
+    for (int x = tid; x < d.S; x += kLmThreads) atomicAdd(&counts[assign[x]], 1);
+    if (!tabled)  // per-update pruning needs every class's eigensystem
+        for (int k = warp; k < K; k += kLmThreads / 32)
             spectral_decompose_warp_ws(base, logits + (size_t)k * kStates, spec + (size_t)k * kSpecStride,
                                        work[warp]);
     __syncthreads();
-    for (int it = 0; it < gp.n_iter; ++it) {
+    bool ok = true;
+    for (int it = 0; it < gp.n_iter && ok; ++it) {
         // One site, uniform over all S. A site alone in its class stays put
         // (the move never empties a class), so the site is selected with
         // probability 1/S both ways and the selection cancels from the
         // Metropolis-Hastings ratio: a draw from only the sites that may move
         // would not, since moving a site changes which sites those are.
-        if (threadIdx.x == 0) {
-            int c = (int)((1.0 - curand_uniform_double(&rng_state)) * d.S);
-            c = c < d.S ? c : d.S - 1;
-            s_site = counts[assign[c]] >= 2 ? c : -1;
+        if (tid == 0) {
+            if (gp.fixed_site >= 0) {  // scores mode
+                s_site = gp.fixed_site;
+            } else {
+                int c = (int)((1.0 - curand_uniform_double(&rng_state)) * d.S);
+                c = c < d.S ? c : d.S - 1;
+                s_site = counts[assign[c]] >= 2 ? c : -1;
+            }
         }
         __syncthreads();
         const int s = s_site;
         if (s < 0) continue;
+        if (tid < kSiteFeat) sfs[tid] = site_feat[(size_t)s * kSiteFeat + tid];
         if (!tabled)
-            for (int c = threadIdx.x; c < d.T; c += blockDim.x) scode[c] = a.codes[(size_t)c * d.S + s];
-        const float* sf = site_feat + (size_t)s * kSiteFeat;
-        for (int k = warp; k < K; k += kGibbsWarps) {  // forward scores
-            mlp_features(sf, spec + (size_t)k * kSpecStride + kSpecPi, counts[k], xs + warp * kMlpIn);
-            const float v = mlp_score(W, xs + warp * kMlpIn, hs + warp * kMlpHid);
-            if (lane == 0) score[k] = v;
-            __syncwarp();
+            for (int c = tid; c < d.T; c += kLmThreads) scode[c] = a.codes[(size_t)c * d.S + s];
+        __syncthreads();
+        // Forward scores, 128 classes per product.
+        for (int rb = 0; rb < K && ok; rb += kLmThreads) {
+            const int k = rb + tid;
+            const bool on = k < K;
+            lm_features(tl, sfs, pis + (size_t)(on ? k : 0) * kStates, lpis + (size_t)(on ? k : 0) * kStates,
+                        on ? counts[k] : 1, on);
+            float v;
+            ok = lm_scores(ls, ok, w1t, w2t, bias, bias + kMlpHid, bias + 2 * kMlpHid, b3, a.status, &v);
+            if (on) score[k] = v;
         }
         __syncthreads();
+        if (!ok) break;
+        if (gp.fixed_site >= 0) {  // scores mode: report the forward scores, move nothing
+            for (int k = tid; k < K; k += kLmThreads) a.weights_out[(size_t)i * (a.Kcap + kAux) + k] = score[k];
+            break;
+        }
         if (warp == 0) {  // the proposal draw, in class order (warp scan over chunks of 32)
             float mx = -INFINITY;
             for (int k = lane; k < K; k += 32) mx = fmaxf(mx, score[k]);
@@ -639,29 +847,35 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
         __syncthreads();
         const int ca = s_a, cb = s_b;
         if (ca == cb) {  // proposing the current class: a no-op, always accepted
-            if (threadIdx.x == 0) acc_n++;
+            if (tid == 0) acc_n++;
             __syncthreads();
             continue;
         }
+        // Reverse scores: the two classes with their sizes after the move, from
+        // the products of their row blocks.
+        for (int pass = 0; pass < 2 && ok; ++pass) {
+            const int rb = (pass == 0 ? ca : cb) / kLmThreads * kLmThreads;
+            if (pass == 1 && rb == ca / kLmThreads * kLmThreads) break;  // same block as ca
+            const int k = rb + tid;
+            const bool on = (k == ca || k == cb);
+            lm_features(tl, sfs, pis + (size_t)(on ? k : 0) * kStates, lpis + (size_t)(on ? k : 0) * kStates,
+                        on ? counts[k] + (k == ca ? -1 : 1) : 1, on);
+            float v;
+            ok = lm_scores(ls, ok, w1t, w2t, bias, bias + kMlpHid, bias + 2 * kMlpHid, b3, a.status, &v);
+            if (k == ca) rev[0] = v;
+            if (k == cb) rev[1] = v;
+        }
         // Without the table: site likelihoods under the two classes (warps
-        // 0..nb-1: a, nb..2nb-1: b, kRateBlockLearned rates each). Reverse
-        // scores with the updated class sizes on the next two warps.
-        const int nb = tabled ? 0 : (d.R + kRateBlockLearned - 1) / kRateBlockLearned;
-        if (warp < 2 * nb) {
-            const int which = warp < nb ? 0 : 1, r0 = (warp % nb) * kRateBlockLearned;
+        // 0..nb-1: a, nb..2nb-1: b, kRateBlock rates each).
+        const int nb = tabled ? 0 : (d.R + kRateBlock - 1) / kRateBlock;
+        if (ok && warp < 2 * nb) {
+            const int which = warp < nb ? 0 : 1, r0 = (warp % nb) * kRateBlock;
             const int k = which == 0 ? ca : cb;
-            site_class_lnl<kRateBlockLearned>(a, gp, i, r0, spec + (size_t)k * kSpecStride, stash, scode,
-                                              xch[warp], lrate[which] + r0);
-        } else if (warp < 2 * nb + 2) {
-            const int w = warp - 2 * nb;
-            const int k = w == 0 ? ca : cb;
-            mlp_features(sf, spec + (size_t)k * kSpecStride + kSpecPi, counts[k] + (w == 0 ? -1 : 1),
-                         xs + warp * kMlpIn);
-            const float v = mlp_score(W, xs + warp * kMlpIn, hs + warp * kMlpHid);
-            if (lane == 0) rev[w] = v;
+            site_class_lnl<kRateBlock>(a, gp, i, r0, spec + (size_t)k * kSpecStride, stash, scode, xch[warp],
+                                       lrate[which] + r0);
         }
         __syncthreads();
-        if (warp == 0) {
+        if (ok && warp == 0) {
             float mx = -INFINITY, mx2 = -INFINITY;
             for (int k = lane; k < K; k += 32) {
                 mx = fmaxf(mx, score[k]);
@@ -696,8 +910,15 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) learned_move_kernel(GibbsArg
         }
         __syncthreads();
     }
-    for (int k = threadIdx.x; k < K; k += blockDim.x) a.counts[(size_t)i * (a.Kcap + kAux) + k] = counts[k];
-    if (threadIdx.x == 0) {
+    // A product still in flight (after a wait gave up) lands before the
+    // tensor memory is released.
+    if (tid == 0 && ls.pend) lm_wait(ls.bar, ls.phase, kDrainPolls);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(ls.tm), "r"(kLmCols) : "memory");
+    for (int k = tid; k < K; k += kLmThreads) a.counts[(size_t)i * (a.Kcap + kAux) + k] = counts[k];
+    if (tid == 0) {
         a.kout[i] = K;
         n_acc[i] = acc_n;
         n_prop[i] = prop_n;
@@ -753,13 +974,12 @@ cudaError_t launch_learned_move(GibbsArgs a, int n_iter, const void* mlp, const 
     const ScratchLayout L = scratch_layout(d, a.count, a.Kcap, n_iter, a.nslots, false);
     a.spec = scratch + L.spec;
     a.stash = scratch + L.stash;
-    const size_t smem = ((kMlpParams * 2 + 15) & ~15) +
-                        sizeof(float) * (kGibbsWarps * (kMlpIn + kMlpHid) + a.Kcap) + sizeof(int) * a.Kcap +
-                        d.T + 16;
+    const size_t smem = kLmW1Bytes + kLmW2Bytes + sizeof(float) * (3 * kMlpHid + (size_t)a.Kcap * (2 * kStates + 1)) +
+                        sizeof(int) * a.Kcap + d.T + 16;
     cudaError_t e = cudaFuncSetAttribute(learned_move_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    learned_move_kernel<<<a.count, 32 * kGibbsWarps, smem, st>>>(
+    learned_move_kernel<<<a.count, kLmThreads, smem, st>>>(
         a, static_cast<const __nv_bfloat16*>(mlp), site_feat, n_acc, n_prop);
     return cudaGetLastError();
 }

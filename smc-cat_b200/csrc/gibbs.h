@@ -45,7 +45,8 @@ struct GibbsArgs {
     const uint8_t* codes;
     const double* isinv;
     const int32_t* invchar;
-    int* status;            // bit 4: class capacity exhausted
+    int* status;            // bit 4: class capacity exhausted; bit 8: a bounded wait gave up
+    uint32_t wait_limit;    // polls per bounded wait
     // Optional [count][Kt][S]: every site's log-likelihood (+I mixed) under each
     // class the particle enters with, evaluated beforehand by the pruning
     // kernels; those classes then need no single-site pruning per iteration.

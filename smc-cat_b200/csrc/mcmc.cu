@@ -1026,6 +1026,7 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         a.isinv = isinv_device(c);
         a.invchar = invchar_device(c);
         a.status = reinterpret_cast<int*>(dbuf + o_status);
+        a.wait_limit = wait_limit_of(c);
         a.table = use_table ? reinterpret_cast<const double*>(dbuf + o_table) : nullptr;
         a.Kt = d.Kmax;
         double* scr = reinterpret_cast<double*>(dbuf + o_scr);
@@ -1095,9 +1096,11 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     if (site >= 0) {
         const int K = slot_of(c, list[0]).cur.K;
         for (int k = 0; k < K; ++k) weights_out[k] = wout[k];
-        for (int j = 0; j < naux; ++j) weights_out[K + j] = wout[K + j];
+        if (learned_updates == 0)
+            for (int j = 0; j < naux; ++j) weights_out[K + j] = wout[K + j];
         return SMCCAT_OK;
     }
+    if (status & 8) return mfail(SMCCAT_ETIMEOUT, "a bounded wait in the learned move gave up");
     if (status & 4) return mfail(SMCCAT_ENOMEM, "Gibbs reassignment ran out of class slots");
     // Compact the surviving classes and install the new assignments
     // (the reference erases empty classes as it goes, Particle.cpp:817-821).
@@ -1163,7 +1166,7 @@ int smccat_learned_move(smccat_ctx* c, int32_t first, int32_t count, const uint8
                         smccat_learned_stats* stats) {
     if (!c || first < 0 || count < 0 || updates < 1) return mfail(SMCCAT_EINVAL, "bad argument");
     if (!(model_flags_of(c) & SMCCAT_MODEL_CAT)) return mfail(SMCCAT_EINVAL, "the learned move needs SMCCAT_MODEL_CAT");
-    if (2 * dims_of(c).R + 2 > 16) return mfail(SMCCAT_EINVAL, "the learned move supports at most 7 rates");
+    if (dims_of(c).R > 2 * 4) return mfail(SMCCAT_EINVAL, "the learned move supports at most 8 rates");
     std::vector<int> list;
     for (int i = 0; i < count; ++i) {
         if (mask && !mask[i]) continue;
@@ -1175,9 +1178,19 @@ int smccat_learned_move(smccat_ctx* c, int32_t first, int32_t count, const uint8
     return run_gibbs(c, list, temperature, seed, -1, nullptr, nullptr, nullptr, updates, stats);
 }
 
+int smccat_learned_scores(smccat_ctx* c, int32_t p, int32_t site, double* out) {
+    if (!c || !out || p < 0 || p >= particles_of(c)) return mfail(SMCCAT_EINVAL, "bad argument");
+    if (!(model_flags_of(c) & SMCCAT_MODEL_CAT)) return mfail(SMCCAT_EINVAL, "the learned move needs SMCCAT_MODEL_CAT");
+    if (dims_of(c).R > 2 * 4) return mfail(SMCCAT_EINVAL, "the learned move supports at most 8 rates");
+    if (site < 0 || site >= dims_of(c).S) return mfail(SMCCAT_EINVAL, "site out of range");
+    const Slot& s = slot_of(c, p);
+    if (!s.loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
+    return run_gibbs(c, {p}, 1.0, 0, site, nullptr, out, nullptr, 1, nullptr);
+}
+
 int smccat_gibbs_weights(smccat_ctx* c, int32_t p, int32_t site, const double* aux_logits,
                          double temperature, double* out) {
-    if (!c || !aux_logits || !out || p < 0) return mfail(SMCCAT_EINVAL, "bad argument");
+    if (!c || !aux_logits || !out || p < 0 || p >= particles_of(c)) return mfail(SMCCAT_EINVAL, "bad argument");
     const Slot& s = slot_of(c, p);
     if (!s.loaded) return mfail(SMCCAT_ESTATE, "particle has no state loaded");
     if (site < 0 || site >= dims_of(c).S) return mfail(SMCCAT_EINVAL, "site out of range");

@@ -154,6 +154,7 @@ def lib():
         "smccat_learned_params": ([vp, _fp, _fp], ctypes.c_int),
         "smccat_learned_move": ([vp, _i32, _i32, _up, _i32, ctypes.c_double, ctypes.c_uint64,
                                  ctypes.POINTER(LearnedStats)], ctypes.c_int),
+        "smccat_learned_scores": ([vp, _i32, _i32, _dp], ctypes.c_int),
         "smccat_get_profile": ([vp, ctypes.POINTER(Profile)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -487,6 +488,12 @@ class Engine:
         _check(lib().smccat_learned_move(self._h, int(first), int(count), mp, int(updates),
                                          float(temperature), int(seed), ctypes.byref(st)))
         return {"proposed": int(st.proposed), "accepted": int(st.accepted)}
+
+    def learned_scores(self, p, site, num_classes) -> np.ndarray:
+        """The learned proposal's score of every class of particle p at `site`."""
+        out = np.zeros(int(num_classes))
+        _check(lib().smccat_learned_scores(self._h, int(p), int(site), out.ctypes.data_as(_dp)))
+        return out
 
     def smc_step(self, raw_weights, target_ess, last_temp, first=0):
         w = np.array(raw_weights, dtype=np.float64, copy=True)

@@ -144,3 +144,56 @@ def test_learned_move_table_matches_per_update_pruning():
     assert prop_a == prop_b and acc_a == acc_b
     np.testing.assert_array_equal(a, b)
     np.testing.assert_allclose(la, lb, rtol=1e-9)
+
+
+def _bf16(x):
+    """Round to the nearest BF16 (ties to even), returned as float32."""
+    a = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((a + 0x7FFF + ((a >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def test_tensor_core_scores_match_cpu_oracle():
+    """The learned move scores every class with two tcgen05 BF16 products
+    (feature rows, weights and hidden activations in BF16, FP32 accumulation).
+    Against the float64 oracle forward pass on the same features, with the same
+    BF16 roundings applied, for a particle with more classes than one 128-row
+    product holds."""
+    K, S, T = 150, 400, 8
+    cfg = workload.WorkloadConfig("scores", T=T, S=S, R=4, particles=1, iterations=1, lg=False,
+                                  invar=False, cat=True, k_range=(K, K), seed=12)
+    rng = np.random.default_rng(12)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    st = workload.make_particles(cfg, 1, rng, kmax=K)
+    eng = smccat.Engine(codes, cfg.R, 1, max_classes=K, cat=True)
+    eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                      st["logits"], st["assign"], st["pinv"], st["shape"])
+    eng.refresh(full=True)
+    params = (np.random.default_rng(6).normal(size=omlp.N_PARAMS) * 0.15).astype(np.float32)
+    eng.learned_params(set_to=params)
+    q = omlp.unpack(_bf16(params).astype(np.float64))
+    lg = st["logits"][0][:K]
+    pi = np.exp(lg - lg.max(axis=1, keepdims=True))
+    pi /= pi.sum(axis=1, keepdims=True)
+    pi32 = pi.astype(np.float32)
+    lpi32 = np.log(pi).astype(np.float32)
+    counts = np.bincount(st["assign"][0], minlength=K)
+    for site in (0, 17, 233, S - 1):
+        col = codes[:, site]
+        res = col[col < 20]
+        sf = np.zeros(21, np.float32)
+        sf[:20] = np.bincount(res, minlength=20)[:20] / max(len(res), 1)
+        sf[20] = 1.0 - len(res) / T
+        X = np.zeros((K, omlp.IN), np.float32)
+        X[:, :21] = sf
+        X[:, 21:41] = pi32
+        X[:, 41] = np.log(np.maximum(counts, 1)).astype(np.float32)
+        X[:, 42] = (lpi32 * sf[:20]).sum(axis=1)
+        Xq = _bf16(X).astype(np.float64)
+        H1 = _bf16(np.maximum(Xq @ q["W1"] + q["b1"], 0)).astype(np.float64)
+        H2 = np.maximum(H1 @ q["W2"] + q["b2"], 0)
+        ref = H2 @ q["w3"] + q["b3"][0]
+        got = eng.learned_scores(0, site, K)
+        scale = np.abs(ref).max()
+        np.testing.assert_allclose(got, ref, atol=3e-3 * scale, rtol=0)
+    eng.close()
