@@ -44,6 +44,15 @@ constexpr int kAuxCtasPerSm = 3;
 // at 64 (kAux + 1). The auxiliary-class kernel and the sequential pass read
 // the same draws, and no draw depends on the chain's state.
 constexpr unsigned long long kOffAux = 64, kOffChoice = 64ull * (kAux + 1);
+// The learned move's update `it` uses the same site draw (offset 0), its
+// proposal draw at kOffProposal and its acceptance draw at kOffAccept.
+constexpr unsigned long long kOffProposal = 64, kOffAccept = 128;
+
+__device__ double draw_at(unsigned long long seed, int p, int it, unsigned long long off) {
+    curandStatePhilox4_32_10_t r;
+    curand_init(seed, ((unsigned long long)p << 24) | (unsigned long long)it, off, &r);
+    return curand_uniform_double(&r);
+}
 
 __device__ __forceinline__ unsigned long long iter_stream(int p, int it) {
     return ((unsigned long long)p << 24) | (unsigned long long)it;
@@ -306,6 +315,52 @@ __global__ void __launch_bounds__(32 * kAuxWarps, kAuxCtasPerSm) gibbs_aux_kerne
         if (lane == 0) a.aux_ls[t] = site_value(a, gp, s, lr[warp], rec + kSpecPi);
         __syncwarp();
     }
+}
+
+// The sites a pass draws, without the rest of the auxiliary work (the learned
+// move, whose site draws come from the same streams).
+__global__ void draw_sites_kernel(GibbsArgs a, int n_iter) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)a.count * n_iter) return;
+    const int it = (int)(t % n_iter), i = (int)(t / n_iter);
+    a.aux_site[t] = draw_site(a.seed, a.parts[i].p, it, a.d.S);
+}
+
+// Particle i's distinct drawn sites in increasing order into row q = qrow[i]
+// of the evaluation site lists (the rest of the row zero) and their count
+// into nv[q]; `flags` is [count][S] scratch. One CTA per particle.
+constexpr int kVisitThreads = 512;
+__global__ void __launch_bounds__(kVisitThreads) visited_sites_kernel(const int32_t* sites, int n_iter,
+                                                                      const int32_t* qrow, int S,
+                                                                      uint8_t* flags, int32_t* list,
+                                                                      int32_t* nv) {
+    const int i = blockIdx.x, tid = threadIdx.x;
+    uint8_t* f = flags + (size_t)i * S;
+    for (int x = tid; x < S; x += kVisitThreads) f[x] = 0;
+    __syncthreads();
+    for (int it = tid; it < n_iter; it += kVisitThreads) f[sites[(size_t)i * n_iter + it]] = 1;
+    __syncthreads();
+    // Contiguous chunks per thread, an exclusive scan of the chunk counts.
+    const int chunk = (S + kVisitThreads - 1) / kVisitThreads;
+    const int x0 = min(S, tid * chunk), x1 = min(S, x0 + chunk);
+    int c = 0;
+    for (int x = x0; x < x1; ++x) c += f[x];
+    __shared__ int part[kVisitThreads];
+    part[tid] = c;
+    __syncthreads();
+    for (int o = 1; o < kVisitThreads; o <<= 1) {
+        const int v = tid >= o ? part[tid - o] : 0;
+        __syncthreads();
+        part[tid] += v;
+        __syncthreads();
+    }
+    int pos = part[tid] - c;
+    int32_t* row = list + (size_t)qrow[i] * S;
+    for (int x = x0; x < x1; ++x)
+        if (f[x]) row[pos++] = x;
+    const int total = part[kVisitThreads - 1];
+    for (int x = total + tid; x < S; x += kVisitThreads) row[x] = 0;
+    if (tid == 0) nv[qrow[i]] = total;
 }
 
 // The sequential part of a Gibbs pass, one CTA per particle over its
@@ -715,7 +770,6 @@ __global__ void __launch_bounds__(kLmThreads) learned_move_kernel(GibbsArgs a, c
     __shared__ double lrate[2][kMaxRates];
     __shared__ float rev[2], sfs[kSiteFeat];
     __shared__ int s_site, s_a, s_b;
-    __shared__ curandStatePhilox4_32_10_t rng_state;
     __shared__ SpecWork work[kLmThreads / 32];
     __shared__ int acc_n, prop_n;
     __shared__ __align__(8) uint64_t mma_bar;
@@ -751,7 +805,6 @@ __global__ void __launch_bounds__(kLmThreads) learned_move_kernel(GibbsArgs a, c
     }
     for (int k = tid; k < a.Kcap; k += kLmThreads) counts[k] = 0;
     if (tid == 0) {
-        curand_init(a.seed, (unsigned long long)gp.p, 0ull, &rng_state);
         acc_n = prop_n = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(lm_sa(&mma_bar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -786,8 +839,7 @@ __global__ void __launch_bounds__(kLmThreads) learned_move_kernel(GibbsArgs a, c
             if (gp.fixed_site >= 0) {  // scores mode
                 s_site = gp.fixed_site;
             } else {
-                int c = (int)((1.0 - curand_uniform_double(&rng_state)) * d.S);
-                c = c < d.S ? c : d.S - 1;
+                const int c = draw_site(a.seed, gp.p, it, d.S);
                 s_site = counts[assign[c]] >= 2 ? c : -1;
             }
         }
@@ -824,7 +876,8 @@ __global__ void __launch_bounds__(kLmThreads) learned_move_kernel(GibbsArgs a, c
                 const double x = warp_incl_scan(k < K ? exp((double)(score[k] - mx)) : 0.0);
                 run += __shfl_sync(0xffffffffu, x, 31);
             }
-            const double u = __shfl_sync(0xffffffffu, lane == 0 ? curand_uniform_double(&rng_state) : 0.0, 0);
+            const double u =
+                __shfl_sync(0xffffffffu, lane == 0 ? draw_at(a.seed, gp.p, it, kOffProposal) : 0.0, 0);
             const double draw = run * u;
             int b = K - 1;
             run = 0.0;
@@ -900,7 +953,7 @@ __global__ void __launch_bounds__(kLmThreads) learned_move_kernel(GibbsArgs a, c
                 // CRP prior ratio n_b / (n_a - 1); tempered likelihood ratio.
                 const double lr = a.temp * (lb - la) + log((double)counts[cb]) -
                                   log((double)(counts[ca] - 1)) + lq_rev - lq_fwd;
-                if (log(curand_uniform_double(&rng_state)) <= lr) {
+                if (log(draw_at(a.seed, gp.p, it, kOffAccept)) <= lr) {
                     assign[s] = cb;
                     counts[ca]--;
                     counts[cb]++;
@@ -968,12 +1021,28 @@ ScratchLayout scratch_layout(const Dims& d, int count, int Kcap, int n_iter, int
 
 }  // namespace
 
+namespace {
+
+void set_scratch(GibbsArgs& a, int n_iter, double* scratch) {
+    const ScratchLayout L = scratch_layout(a.d, a.count, a.Kcap, n_iter, a.nslots, true);
+    a.spec = scratch + L.spec;
+    a.stash = scratch + L.stash;
+    a.aux_ls = scratch + L.aux_ls;
+    a.aux_site = reinterpret_cast<int32_t*>(scratch + L.aux_site);
+    a.aux_rec = scratch + L.aux_rec;
+    a.aux_stash = scratch + L.aux_stash;
+}
+
+size_t gibbs_smem(const GibbsArgs& a) {
+    return sizeof(double) * ((size_t)a.Kcap * a.d.R + a.Kcap + kAux) + sizeof(int) * (a.Kcap + kAux) + a.d.T + 16;
+}
+
+}  // namespace
+
 cudaError_t launch_learned_move(GibbsArgs a, int n_iter, const void* mlp, const float* site_feat,
                                 int32_t* n_acc, int32_t* n_prop, double* scratch, cudaStream_t st) {
     const Dims& d = a.d;
-    const ScratchLayout L = scratch_layout(d, a.count, a.Kcap, n_iter, a.nslots, false);
-    a.spec = scratch + L.spec;
-    a.stash = scratch + L.stash;
+    set_scratch(a, n_iter, scratch);
     const size_t smem = kLmW1Bytes + kLmW2Bytes + sizeof(float) * (3 * kMlpHid + (size_t)a.Kcap * (2 * kStates + 1)) +
                         sizeof(int) * a.Kcap + d.T + 16;
     cudaError_t e = cudaFuncSetAttribute(learned_move_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -984,46 +1053,46 @@ cudaError_t launch_learned_move(GibbsArgs a, int n_iter, const void* mlp, const 
     return cudaGetLastError();
 }
 
-cudaError_t launch_gibbs_resume(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st) {
-    const Dims& d = a.d;
-    const ScratchLayout L = scratch_layout(d, a.count, a.Kcap, n_iter, a.nslots, true);
-    a.spec = scratch + L.spec;
-    a.stash = scratch + L.stash;
-    a.aux_ls = scratch + L.aux_ls;
-    a.aux_site = reinterpret_cast<int32_t*>(scratch + L.aux_site);
-    a.aux_rec = scratch + L.aux_rec;
-    a.aux_stash = scratch + L.aux_stash;
-    const size_t smem = sizeof(double) * ((size_t)a.Kcap * d.R + a.Kcap + kAux) +
-                        sizeof(int) * (a.Kcap + kAux) + d.T + 16;
-    gibbs_kernel<<<a.count, 32 * kGibbsWarps, smem, st>>>(a);
-    return cudaGetLastError();
-}
-
 size_t gibbs_scratch_doubles(const Dims& d, int count, int Kcap, int n_iter, int nslots, bool aux) {
     return scratch_layout(d, count, Kcap, n_iter, nslots, aux).total;
 }
 
 int gibbs_aux() { return kAux; }
 
-cudaError_t launch_gibbs(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st) {
-    const Dims& d = a.d;
-    const ScratchLayout L = scratch_layout(d, a.count, a.Kcap, n_iter, a.nslots, true);
-    a.spec = scratch + L.spec;
-    a.stash = scratch + L.stash;
-    a.aux_ls = scratch + L.aux_ls;
-    a.aux_site = reinterpret_cast<int32_t*>(scratch + L.aux_site);
-    a.aux_rec = scratch + L.aux_rec;
-    a.aux_stash = scratch + L.aux_stash;
+cudaError_t launch_gibbs_aux(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st) {
+    set_scratch(a, n_iter, scratch);
     const size_t tasks = (size_t)a.count * n_iter * kAux;
-    gibbs_aux_kernel<<<aux_grid(tasks), 32 * kAuxWarps, (size_t)kAuxWarps * d.T, st>>>(a, n_iter);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    const size_t smem = sizeof(double) * ((size_t)a.Kcap * d.R + a.Kcap + kAux) +
-                        sizeof(int) * (a.Kcap + kAux) + d.T + 16;
-    e = cudaFuncSetAttribute(gibbs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    gibbs_aux_kernel<<<aux_grid(tasks), 32 * kAuxWarps, (size_t)kAuxWarps * a.d.T, st>>>(a, n_iter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_draw_sites(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st) {
+    set_scratch(a, n_iter, scratch);
+    const size_t n = (size_t)a.count * n_iter;
+    draw_sites_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, n_iter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_visited_sites(GibbsArgs a, int n_iter, double* scratch, const int32_t* qrow, uint8_t* flags,
+                                 int32_t* list, int32_t* nv, cudaStream_t st) {
+    set_scratch(a, n_iter, scratch);
+    visited_sites_kernel<<<a.count, kVisitThreads, 0, st>>>(a.aux_site, n_iter, qrow, a.d.S, flags, list, nv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gibbs_resume(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st) {
+    set_scratch(a, n_iter, scratch);
+    const size_t smem = gibbs_smem(a);
+    cudaError_t e = cudaFuncSetAttribute(gibbs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     gibbs_kernel<<<a.count, 32 * kGibbsWarps, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t launch_gibbs(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st) {
+    cudaError_t e = launch_gibbs_aux(a, n_iter, scratch, st);
+    if (e == cudaSuccess) e = launch_gibbs_resume(a, n_iter, scratch, st);
+    return e;
 }
 
 }  // namespace smccat

@@ -80,8 +80,17 @@ int gibbs_aux();
 // A Gibbs pass: the auxiliary-class kernel (every iteration's drawn site and
 // auxiliary classes, all at once), then one sequential CTA per particle.
 cudaError_t launch_gibbs(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st);
-// The next round of a table-mode pass (the sequential kernel alone).
+// Its two parts: the auxiliary-class kernel, and one round of the sequential
+// kernel (table mode runs it until no particle stops at a new class).
+cudaError_t launch_gibbs_aux(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st);
 cudaError_t launch_gibbs_resume(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st);
+// The sites a learned-move pass draws (into the scratch's drawn-site array).
+cudaError_t launch_draw_sites(GibbsArgs a, int n_iter, double* scratch, cudaStream_t st);
+// Each particle's distinct drawn sites in increasing order into row qrow[i] of
+// the evaluation site lists `list` [rows][S] (the rest of the row zero), their
+// count into nv[qrow[i]]; flags: [count][S] bytes of scratch.
+cudaError_t launch_visited_sites(GibbsArgs a, int n_iter, double* scratch, const int32_t* qrow, uint8_t* flags,
+                                 int32_t* list, int32_t* nv, cudaStream_t st);
 
 // Learned-proposal MH site reassignment: parts[i].n_iter updates per particle
 // among its existing classes, proposals from the scoring MLP (BF16 weights

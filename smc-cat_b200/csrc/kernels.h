@@ -66,6 +66,13 @@ struct PruneArgs {
     // eval_kp[p - first] (any slot below Kmax whose matrices and spectral
     // record are in place; -1 skips the particle) and eval_k is not used.
     const int32_t* eval_kp = nullptr;
+    // Evaluation over site lists: when set, slot j of particle p's tiles stands
+    // for site eval_perm[(p - first) S + j] and slots at or past
+    // eval_nv[p - first] are not evaluated. The tiles keep the committed
+    // layout's columns, so each column's free workspace is the one its own
+    // class's flips name.
+    const int32_t* eval_perm = nullptr;
+    const int32_t* eval_nv = nullptr;
 };
 
 cudaError_t launch_spec(const SpecJob* jobs, int n, double* spec, const Dims& d, cudaStream_t st);

@@ -293,16 +293,24 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     __shared__ int bad;
 
     const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
-    const bool valid = lane < tl.nslots;  // the lane owns at least one slot
+    // The class whose matrices and frequencies the tile runs: its own, or the
+    // class under evaluation.
+    const int ek = a.eval_kp ? a.eval_kp[p - a.first] : a.eval_k;
+    const int kc = ek >= 0 ? ek : tl.k;
+    // Evaluation over a site list: the tile's slots stand for listed sites.
+    const bool listed = ek >= 0 && a.eval_perm != nullptr;
+    const int nsl = listed ? min(tl.nslots, a.eval_nv[p - a.first] - tl.slot0) : tl.nslots;
+    const int32_t* sperm = listed ? a.eval_perm + (size_t)(p - a.first) * d.S : a.perm + (size_t)p * d.S;
+    const bool valid = lane < nsl;  // the lane owns at least one slot
     // A lane's unused slots alias its first slot (or the tile's first): they
     // are computed like the others and never stored.
     bool vw[W];
     int site[W], col[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) {
-        vw[w] = lane + 32 * w < tl.nslots;
+        vw[w] = lane + 32 * w < nsl;
         const int slot = tl.slot0 + (vw[w] ? lane + 32 * w : (valid ? lane : 0));
-        site[w] = a.perm[(size_t)p * d.S + slot];
+        site[w] = sperm[slot];
         col[w] = r * d.Spad + slot;
     }
     T* buf = reinterpret_cast<T*>(smem_raw) + (size_t)r * 4 * kPBlock;
@@ -320,10 +328,6 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     const size_t lws_stride = j_stride;
     T* CLp = static_cast<T*>(a.CL) + (size_t)p * d.NI * node_stride;
     double* LSCp = a.LSC + (size_t)p * d.NI * 2 * lws_stride;
-    // The class whose matrices and frequencies the tile runs: its own, or the
-    // class under evaluation.
-    const int ek = a.eval_kp ? a.eval_kp[p - a.first] : a.eval_k;
-    const int kc = ek >= 0 ? ek : tl.k;
     const T* Pcls = static_cast<const T*>(a.Pm) +
                     ((size_t)p * d.Kmax + kc) * d.N * 2 * (size_t)R * kPBlock + (size_t)r * kPBlock;
     auto pblock = [&](int child, int pws) {
@@ -341,6 +345,7 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     const int ej = ek >= 0 ? a.eval_map[p - a.first] : 0;
     if (a.eval_kp ? (ek < 0 || ej < 0) : (ek >= 0 && (ej < 0 || ek >= h->num_classes)))
         return true;  // uniform as well
+    if (ek >= 0 && nsl <= 0) return true;  // past the end of the site list
 
     // A class-local refresh of another class leaves this tile's partials as
     // they are: only its root reduction reruns. In evaluation mode the plan

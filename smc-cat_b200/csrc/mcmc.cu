@@ -916,7 +916,7 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     // Device buffers for this call (inputs, outputs and kernel scratch).
     const int n_iter = parts[0].n_iter;
     if (n_iter >= (1 << 24)) return mfail(SMCCAT_EINVAL, "too many site iterations in one call");
-    const size_t scratch = gibbs_scratch_doubles(d, n, Kcap, n_iter, nslots, learned_updates == 0);
+    const size_t scratch = gibbs_scratch_doubles(d, n, Kcap, n_iter, nslots, true);
     size_t bytes = 0;
     auto carve = [&](size_t b) { const size_t o = bytes; bytes += (b + 255) & ~size_t(255); return o; };
     const size_t o_parts = carve(sizeof(GibbsPart) * n), o_tree = carve(tree.size() * sizeof(GibbsNode)),
@@ -936,11 +936,20 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     size_t o_rit = 0, o_rk = 0, o_born = 0, o_pjobs = 0, o_pmjobs = 0, o_ekp = 0;
     std::vector<int32_t> rit(n, 0), rk(n), born(n, -1);
     std::vector<PJob> pjobs;
+    // Table mode also lists each particle's drawn sites (the table is filled
+    // for those only): row qrow[j] = list[j] - first of [prange][S].
+    size_t o_qrow = 0, o_flags = 0, o_elist = 0, o_env = 0;
+    std::vector<int32_t> qrow(n);
+    for (int j = 0; j < n; ++j) qrow[j] = list[j] - pfirst;
     if (use_table) {
         o_ehdr = carve(sizeof(PartHdr) * ehdr.size());
         o_enodes = carve(sizeof(NodeJob) * enodes.size());
         o_emap = carve(4 * emap.size());
         o_table = carve((size_t)n * d.Kmax * d.S * 8);
+        o_qrow = carve((size_t)n * 4);
+        o_flags = carve((size_t)n * d.S);
+        o_elist = carve((size_t)prange * d.S * 4);
+        o_env = carve((size_t)prange * 4);
     }
     if (rounds) {
         o_rit = carve((size_t)n * 4);
@@ -998,10 +1007,11 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
         pa.nodes = reinterpret_cast<const NodeJob*>(dbuf + o_enodes);
         pa.eval_map = reinterpret_cast<const int32_t*>(dbuf + o_emap);
         pa.eval_out = reinterpret_cast<double*>(dbuf + o_table);
-        for (int k = 0; k < kmax_list && e == cudaSuccess; ++k) {
-            pa.eval_k = k;
-            e = launch_prune(pa, view.ntiles, view.variant, st);
-        }
+        pa.eval_perm = reinterpret_cast<const int32_t*>(dbuf + o_elist);
+        pa.eval_nv = reinterpret_cast<const int32_t*>(dbuf + o_env);
+        up(o_qrow, qrow.data(), (size_t)n * 4);
+        if (e == cudaSuccess) e = cudaMemsetAsync(dbuf + o_elist, 0, (size_t)prange * d.S * 4, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(dbuf + o_env, 0, (size_t)prange * 4, st);
     }
     if (e == cudaSuccess) {
         GibbsArgs a{};
@@ -1037,11 +1047,30 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
             a.eng_spec = const_cast<double*>(view.spec);
             a.eng_sws = view.sws;
         }
-        if (learned_updates > 0)
-            e = launch_learned_move(a, n_iter, mlp, site_feat, reinterpret_cast<int32_t*>(dbuf + o_acc),
-                                    reinterpret_cast<int32_t*>(dbuf + o_prop), scr, st);
-        else
-            e = launch_gibbs(a, n_iter, scr, st);
+        if (use_table) {
+            // The pass's drawn sites first (they do not depend on the chain),
+            // then the table for those sites only, then the pass.
+            e = learned_updates > 0 ? launch_draw_sites(a, n_iter, scr, st) : launch_gibbs_aux(a, n_iter, scr, st);
+            if (e == cudaSuccess)
+                e = launch_visited_sites(a, n_iter, scr, reinterpret_cast<const int32_t*>(dbuf + o_qrow),
+                                         reinterpret_cast<uint8_t*>(dbuf + o_flags),
+                                         reinterpret_cast<int32_t*>(dbuf + o_elist),
+                                         reinterpret_cast<int32_t*>(dbuf + o_env), st);
+            for (int k = 0; k < kmax_list && e == cudaSuccess; ++k) {
+                pa.eval_k = k;
+                e = launch_prune(pa, view.ntiles, view.variant, st);
+            }
+            pa.eval_k = -1;
+        }
+        if (e == cudaSuccess) {
+            if (learned_updates > 0)
+                e = launch_learned_move(a, n_iter, mlp, site_feat, reinterpret_cast<int32_t*>(dbuf + o_acc),
+                                        reinterpret_cast<int32_t*>(dbuf + o_prop), scr, st);
+            else if (use_table)
+                e = launch_gibbs_resume(a, n_iter, scr, st);
+            else
+                e = launch_gibbs(a, n_iter, scr, st);
+        }
         // Rounds: the classes the last round opened into table slots get
         // their transition matrices and table columns (the pruning kernels'
         // evaluation mode, one class per particle), then the particles resume.
