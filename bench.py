@@ -87,7 +87,51 @@ def parse():
     ap.add_argument("--gibbs-particles", type=int, default=0,
                     help="particles of a CAT --extra-configs run timed through one Gibbs pass "
                          "and one learned-proposal pass (0 to skip)")
+    ap.add_argument("--reassign", type=int, default=0,
+                    help="only time the CAT reassignment passes on --sampler-config with this many "
+                         "particles (FP64 Gibbs, FP32 learned proposal; two passes each) and print "
+                         "that line")
     return ap.parse_args()
+
+
+def measure_reassign_only(cid, n, local, torch, reps=2):
+    """Reassignment passes alone on a CAT configuration, from the sampler
+    comparison's start (its particles and class headroom): `reps` FP64 Gibbs
+    passes, then on an FP32 context one Gibbs warm-up pass, one epoch of MLP
+    training (untimed) and `reps` learned-proposal passes of floor(S/2) updates
+    per particle. Wall clock around device-synchronised calls."""
+    import smccat
+    from smccat import workload
+    cfg = workload.CONFIGS[cid]
+    codes, _ = workload.simulate_alignment(cfg, np.random.default_rng(cfg.seed))
+    st = workload.make_particles(cfg, n, np.random.default_rng(cfg.seed * 7 + 1))
+    kmax = st["logits"].shape[1] + 96
+    logits = np.zeros((n, kmax, 20))
+    logits[:, :st["logits"].shape[1]] = st["logits"]
+    out = {"workload": cfg.name, "particles": n, "site_iterations_per_particle": cfg.S // 2}
+    for arm, prec in (("gibbs_fp64", smccat.PREC_FP64), ("learned_fp32", smccat.PREC_FP32)):
+        eng = smccat.Engine(codes, cfg.R, n, max_classes=kmax, lg=cfg.lg, invar=cfg.invar,
+                            cat=cfg.cat, device=local, precision=prec)
+        eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"], logits,
+                          st["assign"], st["pinv"], st["shape"])
+        eng.refresh(full=True)
+        if arm == "learned_fp32":
+            eng.gibbs(temperature=1.0, seed=1)
+            eng.learned_train(epochs=1, batch_sites=512, lr=1e-3, seed=2, first=0, count=min(n, 8))
+        torch.cuda.synchronize()
+        secs, info = [], []
+        for rep in range(reps):
+            t0 = time.perf_counter()
+            if arm == "gibbs_fp64":
+                r = eng.gibbs(temperature=1.0, seed=200 + rep)
+            else:
+                r = eng.learned_move(updates=cfg.S // 2, temperature=1.0, seed=300 + rep)
+            torch.cuda.synchronize()
+            secs.append(time.perf_counter() - t0)
+            info.append(r)
+        out[arm] = {"seconds": secs, "stats": info}
+        eng.close()
+    return out
 
 
 def algorithmic_cost(T: int, R: int, w: int = 8):
@@ -624,6 +668,13 @@ def main():
     from smccat import workload
 
     torch.cuda.set_device(local)
+    if args.reassign > 0:
+        if rank == 0:
+            print(json.dumps({"metric": "CAT reassignment pass seconds", "unit": "s",
+                              "higher_is_better": False, "data": "synthetic",
+                              "reassign": measure_reassign_only(args.sampler_config, args.reassign,
+                                                                local, torch)}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime

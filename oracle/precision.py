@@ -16,7 +16,12 @@ arithmetic can be measured against FP64 on the same state:
             lo = x - hi read truncated as a tensor core reads an FP32 operand;
   "tf32x3raw" the FP32 operand itself as hi (read truncated), lo likewise:
             both parts cut toward zero;
-  "bf16"    BF16 operands, one product, FP32 accumulation.
+  "bf16"    BF16 operands, one product, FP32 accumulation;
+  "fp16x3"  the split with FP16 parts (hi = x rounded to FP16, lo = the
+            rounded remainder; FP16's 5-bit exponent flushes small entries
+            and remainders to subnormals or zero) -- the kind::f16 form,
+            twice the TF32 MMA rate;
+  "fp16"    FP16 operands, one product, FP32 accumulation.
 
 Rescaling is by exact powers of two and the log-scalers and root sums are
 FP64 in every mode, as in the engine's kernels; only the node products and the
@@ -30,7 +35,7 @@ import numpy as np
 
 import oracle
 
-MODES = ("fp64", "fp32", "tf32x3", "tf32x3raw", "bf16x3", "bf16")
+MODES = ("fp64", "fp32", "tf32x3", "tf32x3raw", "bf16x3", "bf16", "fp16x3", "fp16")
 
 
 def bf16_round(x: np.ndarray) -> np.ndarray:
@@ -65,11 +70,24 @@ def _split_tf32(x: np.ndarray, raw: bool = False):
     return hi, lo
 
 
-def _split(x: np.ndarray):
+def fp16_round(x: np.ndarray) -> np.ndarray:
+    """Round FP32 values to the nearest FP16 (ties to even, subnormals kept,
+    no overflow for the [0, 1] values of partials and matrices), as FP32."""
+    return np.asarray(x, dtype=np.float32).astype(np.float16).astype(np.float32)
+
+
+def _split(x: np.ndarray, rnd=bf16_round):
     x = x.astype(np.float32)
-    hi = bf16_round(x)
-    lo = bf16_round(x - hi)
+    hi = rnd(x)
+    lo = rnd(x - hi)
     return hi, lo
+
+
+def _parts(x: np.ndarray, mode: str):
+    """hi, lo operand parts of a split mode (lo unused by the one-product modes)."""
+    if mode.startswith("tf32"):
+        return _split_tf32(x, mode == "tf32x3raw")
+    return _split(x, fp16_round if mode.startswith("fp16") else bf16_round)
 
 
 def _fma32(a, b, c):
@@ -104,10 +122,9 @@ def _product(P: np.ndarray, X: np.ndarray, mode: str) -> np.ndarray:
             s1 = _fma32(off[:, j + 1:j + 2], X32[j + 1][None, :], s1)
         acc = (s0.astype(np.float64) + s1).astype(np.float32)
     else:
-        tf = mode.startswith("tf32")
-        Oh, Ol = _split_tf32(off, mode == "tf32x3raw") if tf else _split(off)
-        Xh, Xl = _split_tf32(X32, mode == "tf32x3raw") if tf else _split(X32)
-        terms = [(Oh, Xh)] if mode == "bf16" else [(Oh, Xh), (Oh, Xl), (Ol, Xh)]
+        Oh, Ol = _parts(off, mode)
+        Xh, Xl = _parts(X32, mode)
+        terms = [(Oh, Xh)] if mode in ("bf16", "fp16") else [(Oh, Xh), (Oh, Xl), (Ol, Xh)]
         for A, B in terms:
             for j in range(20):
                 acc = _fma32(A[:, j:j + 1], B[j][None, :], acc)
@@ -123,9 +140,8 @@ def _column(P: np.ndarray, codes: np.ndarray, mode: str) -> np.ndarray:
         if mode == "fp32":
             Pc = P32
         else:
-            tf = mode.startswith("tf32")
-            Ph, Pl = _split_tf32(P32, mode == "tf32x3raw") if tf else _split(P32)
-            Pc = Ph if mode == "bf16" else Ph + Pl
+            Ph, Pl = _parts(P32, mode)
+            Pc = Ph if mode in ("bf16", "fp16") else Ph + Pl
     full = np.concatenate([Pc, Pc.sum(axis=1, keepdims=True)], axis=1)  # col 20 = row sums
     return full[:, np.minimum(codes, 20)]
 

@@ -4,8 +4,8 @@
 The FP64 restatement in oracle/precision.py must equal the oracle; then the
 FP32 form in the engine's summation order and the split hi + lo TF32 form
 must stay far inside the 1e-3 |delta lnL| budget, while the split hi + lo BF16
-form loses more than an order of magnitude of accuracy to them, and plain
-BF16 misses the budget outright. (The engine's FP32 kernel is measured on the GPU against
+form loses more than an order of magnitude of accuracy to them, split FP16
+loses more still, and plain BF16 misses the budget outright. (The engine's FP32 kernel is measured on the GPU against
 FP64 by test_gpu_parity.py; this file pins the arithmetic comparison between
 the tensor-core forms.)"""
 import numpy as np
@@ -41,3 +41,16 @@ def test_precision_forms_order():
     # Reading the raw FP32 operand as the hi part truncates both parts toward
     # zero: a one-signed error that ends up worse than split BF16.
     assert r["tf32x3raw"] > r["bf16x3"]
+    # Split FP16 (the kind::f16 form) has TF32's significand but a 5-bit
+    # exponent: small partial entries and the lo remainders fall into FP16's
+    # subnormals or to zero, and the split ends up worse than split BF16.
+    assert r["fp16x3"] > r["bf16x3"]
+    assert r["fp16x3"] > 1e-3
+
+
+def test_fp16_rounding_keeps_subnormals_and_flushes_below():
+    x = np.array([1.0, 1.0 + 2.0 ** -11, 1e-5, 2.0 ** -25, 2.0 ** -26], dtype=np.float32)
+    got = precision.fp16_round(x)
+    assert got[0] == 1.0 and got[1] == 1.0           # tie to even
+    assert abs(got[2] - x[2]) <= 2.0 ** -25           # a subnormal: absolute spacing 2^-24
+    assert got[3] == 0.0 and got[4] == 0.0            # half the smallest subnormal and below: zero
