@@ -626,13 +626,19 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
 }
 
 // One warp per (particle, class) slot: re-decompose the classes a step's
-// proposal marked, into the spectral workspace the proposal switched them to.
+// proposal marked, into the spectral workspace the proposal switched them to,
+// starting from the committed record in the other workspace (the same class
+// before the proposal's small change).
 __global__ void __launch_bounds__(32) dm_spec_kernel(DmArgs a) {
     const int i = blockIdx.x / a.d.Kmax, k = blockIdx.x - i * a.d.Kmax;
     if (!a.spec_flip[(size_t)i * a.d.Kmax + k]) return;
     const size_t pk = (size_t)(a.first + i) * a.d.Kmax + k;
-    double* rec = const_cast<double*>(a.spec) + (pk * 2 + (a.sws[pk] & kSwsSpec)) * kSpecStride;
-    spectral_decompose_warp(a.base + (size_t)i * kBase, a.logits + ((size_t)i * a.d.Kmax + k) * kStates, rec);
+    const int half = a.sws[pk] & kSwsSpec;
+    double* spec = const_cast<double*>(a.spec);
+    __shared__ SpecWork w;
+    spectral_decompose_warp_warm(a.base + (size_t)i * kBase, a.logits + ((size_t)i * a.d.Kmax + k) * kStates,
+                                 spec + (pk * 2 + (half ^ 1)) * kSpecStride, spec + (pk * 2 + half) * kSpecStride,
+                                 w);
 }
 
 // One warp per particle: lane 0 draws the decision, the lanes commit the

@@ -29,22 +29,13 @@ struct SpecWork {
     int pp[10], qq[10];
 };
 
-// Run by exactly one full warp with its own workspace `w`; `rec` holds
-// kSpecStride doubles.
-static __device__ __noinline__ void spectral_decompose_warp_ws(const double* __restrict__ base,
-                                                               const double* __restrict__ logits,
-                                                               double* __restrict__ rec,
-                                                               SpecWork& w) {
+// The symmetrised matrix S of a class into w.A (with w.pi, w.sq).
+static __device__ __forceinline__ void spec_build(const double* __restrict__ base,
+                                                  const double* __restrict__ logits, SpecWork& w) {
     const int lane = threadIdx.x & 31;
     double(&A)[kStates][kStates + 1] = w.A;
-    double(&V)[kStates][kStates + 1] = w.V;
     double(&pi)[kStates] = w.pi;
     double(&sq)[kStates] = w.sq;
-    double(&cs)[10] = w.cs;
-    double(&sn)[10] = w.sn;
-    int(&pp)[10] = w.pp;
-    int(&qq)[10] = w.qq;
-
     double e = (lane < kStates) ? exp(logits[lane]) : 0.0;
     const double tot = warp_sum(e);
     if (lane < kStates) { pi[lane] = e / tot; sq[lane] = sqrt(pi[lane]); }
@@ -78,10 +69,19 @@ static __device__ __noinline__ void spectral_decompose_warp_ws(const double* __r
         }
     }
     if (lane < kStates) A[lane][lane] = diag / mean;
-    for (int idx = lane; idx < kStates * kStates; idx += 32)
-        V[idx / kStates][idx % kStates] = (idx / kStates == idx % kStates) ? 1.0 : 0.0;
     __syncwarp();
+}
 
+// Round-robin Jacobi rotations on w.A, accumulated into w.V, until the
+// off-diagonal mass is below 1e-34 of the diagonal's (at most 40 sweeps).
+static __device__ __forceinline__ void spec_jacobi(SpecWork& w) {
+    const int lane = threadIdx.x & 31;
+    double(&A)[kStates][kStates + 1] = w.A;
+    double(&V)[kStates][kStates + 1] = w.V;
+    double(&cs)[10] = w.cs;
+    double(&sn)[10] = w.sn;
+    int(&pp)[10] = w.pp;
+    int(&qq)[10] = w.qq;
     for (int sweep = 0; sweep < 40; ++sweep) {
         double off = 0.0, dg = 0.0;
         for (int idx = lane; idx < kStates * kStates; idx += 32) {
@@ -140,15 +140,76 @@ static __device__ __noinline__ void spectral_decompose_warp_ws(const double* __r
             __syncwarp();
         }
     }
+}
+
+// The record: lambda, L = D^-1/2 V, Rm = V^T D^1/2 and pi.
+static __device__ __forceinline__ void spec_store(const SpecWork& w, double* __restrict__ rec) {
+    const int lane = threadIdx.x & 31;
     if (lane < kStates) {
-        rec[kSpecLam + lane] = A[lane][lane];
-        rec[kSpecPi + lane] = pi[lane];
+        rec[kSpecLam + lane] = w.A[lane][lane];
+        rec[kSpecPi + lane] = w.pi[lane];
     }
     for (int idx = lane; idx < kStates * kStates; idx += 32) {
         const int i = idx / kStates, m = idx % kStates;
-        rec[kSpecL + i * kStates + m] = V[i][m] / sq[i];   // L[i][m]
-        rec[kSpecRm + m * kStates + i] = V[i][m] * sq[i];  // Rm[m][i]
+        rec[kSpecL + i * kStates + m] = w.V[i][m] / w.sq[i];   // L[i][m]
+        rec[kSpecRm + m * kStates + i] = w.V[i][m] * w.sq[i];  // Rm[m][i]
     }
+}
+
+// Run by exactly one full warp with its own workspace `w`; `rec` holds
+// kSpecStride doubles.
+static __device__ __noinline__ void spectral_decompose_warp_ws(const double* __restrict__ base,
+                                                               const double* __restrict__ logits,
+                                                               double* __restrict__ rec,
+                                                               SpecWork& w) {
+    const int lane = threadIdx.x & 31;
+    spec_build(base, logits, w);
+    for (int idx = lane; idx < kStates * kStates; idx += 32)
+        w.V[idx / kStates][idx % kStates] = (idx / kStates == idx % kStates) ? 1.0 : 0.0;
+    __syncwarp();
+    spec_jacobi(w);
+    spec_store(w, rec);
+}
+
+// The same decomposition started from the eigenvectors of `prev`, the record
+// of a nearby class (the class before a proposal changed its frequencies or
+// exchangeabilities): with U = D_prev^1/2 L_prev (orthogonal), the rotations
+// start from A = U^T S U, nearly diagonal, and V = U, so they converge in a few
+// sweeps instead of from the identity. `rec` (not `prev`) doubles as scratch.
+static __device__ __noinline__ void spectral_decompose_warp_warm(const double* __restrict__ base,
+                                                                 const double* __restrict__ logits,
+                                                                 const double* __restrict__ prev,
+                                                                 double* __restrict__ rec, SpecWork& w) {
+    const int lane = threadIdx.x & 31;
+    spec_build(base, logits, w);
+    for (int idx = lane; idx < kStates * kStates; idx += 32) {
+        const int i = idx / kStates, m = idx % kStates;
+        w.V[i][m] = sqrt(prev[kSpecPi + i]) * prev[kSpecL + idx];
+    }
+    __syncwarp();
+    double* B = rec + kSpecL;  // S U, row-major, until the record is written
+    for (int idx = lane; idx < kStates * kStates; idx += 32) {
+        const int i = idx / kStates, m = idx % kStates;
+        double acc = 0.0;
+        for (int j = 0; j < kStates; ++j) acc = fma(w.A[i][j], w.V[j][m], acc);
+        B[idx] = acc;
+    }
+    __syncwarp();
+    for (int idx = lane; idx < kStates * kStates; idx += 32) {  // U^T (S U), upper triangle
+        const int m = idx / kStates, n = idx % kStates;
+        if (m > n) continue;
+        double acc = 0.0, acc2 = 0.0;
+        for (int i = 0; i < kStates; ++i) {
+            acc = fma(w.V[i][m], B[i * kStates + n], acc);
+            acc2 = fma(w.V[i][n], B[i * kStates + m], acc2);
+        }
+        const double v = 0.5 * (acc + acc2);  // exactly symmetric
+        w.A[m][n] = v;
+        w.A[n][m] = v;
+    }
+    __syncwarp();
+    spec_jacobi(w);
+    spec_store(w, rec);
 }
 
 // For kernels whose blocks are a single decomposing warp.
