@@ -461,7 +461,9 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=10, chosen_sweeps=
 
 def measure_smc(reps, n, local, torch):
     """Whole SMC analyses (main.cpp:147-336 through smccat.smc.run) from the
-    same initial population, per arm and replicate seed: log marginal
+    same initial population, per arm and replicate seed (plain: FP64, host
+    lockstep rejuvenation, Gibbs; chosen: FP32, the device sweep, the learned
+    proposal with Gibbs every 4th round): log marginal
     likelihood, SMC steps, resampling rounds, wall seconds, final ESS per
     second. The initial population comes from the workload generator, not
     from the prior, so log Z is compared between arms, not to a truth."""
@@ -477,8 +479,8 @@ def measure_smc(reps, n, local, torch):
     logits[:, :st["logits"].shape[1]] = st["logits"]
     out = {"workload": cfg.name, "particles": n, "rejuvenation_iterations": cfg.iterations,
            "threshold": 0.6, "alg8_probability": 0.1}
-    for arm, prec, move in (("plain_fp64_gibbs", smccat.PREC_FP64, "gibbs"),
-                            ("fp32_learned", smccat.PREC_FP32, "learned")):
+    for arm, prec, move, dev in (("plain_fp64_gibbs", smccat.PREC_FP64, "gibbs", False),
+                                 ("fp32_learned", smccat.PREC_FP32, "learned", True)):
         runs = []
         for r in range(reps):
             eng = smccat.Engine(codes, cfg.R, n, max_classes=kmax, lg=cfg.lg, invar=cfg.invar,
@@ -487,7 +489,7 @@ def measure_smc(reps, n, local, torch):
                               logits, st["assign"], st["pinv"], st["shape"])
             eng.refresh(full=True)
             res = smc.run(eng, cat=True, iterations=cfg.iterations, reassign=move, seed=1000 + r,
-                          sync=torch.cuda.synchronize)
+                          sync=torch.cuda.synchronize, device_sweep=dev)
             res.pop("temperatures")
             runs.append(res)
             eng.close()
@@ -497,6 +499,12 @@ def measure_smc(reps, n, local, torch):
                     "seconds_mean": float(np.mean([x["seconds"] for x in runs])),
                     "final_ess_per_s_mean": float(np.mean([x["final_ess_per_s"] for x in runs]))}
     out["speedup_wall"] = out["plain_fp64_gibbs"]["seconds_mean"] / out["fp32_learned"]["seconds_mean"]
+    # Paired by replicate seed (the same initial population and SMC seed per pair).
+    d = np.array([a["log_z"] - b["log_z"] for a, b in zip(out["fp32_learned"]["runs"],
+                                                           out["plain_fp64_gibbs"]["runs"])])
+    out["log_z_paired_difference"] = {
+        "mean": float(d.mean()), "sd": float(d.std(ddof=1)) if reps > 1 else None,
+        "standard_error": float(d.std(ddof=1) / np.sqrt(reps)) if reps > 1 else None}
     return out
 
 

@@ -35,9 +35,12 @@ def _lse(x: np.ndarray) -> float:
 def run(eng, *, cat: bool, iterations: int = 20, threshold: float = 0.6,
         alg8_probability: float = 0.1, reassign: str = "gibbs", learned_warmup: int = 2,
         learned_updates: int | None = None, gibbs_every: int = 4, seed: int = 0,
-        max_steps: int = 100000, sync=None) -> dict:
+        max_steps: int = 100000, sync=None, device_sweep: bool = False) -> dict:
     """Run the loop on all of ``eng``'s particles (loaded and refreshed).
-    ``sync`` (optional) is called before reading the wall clock."""
+    ``sync`` (optional) is called before reading the wall clock.
+    ``device_sweep``: rejuvenate with the whole Mcmc::operator() sweep on the
+    device (one CUDA graph, ``Engine.mcmc_sweep``) instead of the host-driven
+    lockstep (``Engine.rejuvenate``)."""
     n = eng.P
     rng = np.random.default_rng(seed)
     raw = np.full(n, -np.log(n))
@@ -58,8 +61,8 @@ def run(eng, *, cat: bool, iterations: int = 20, threshold: float = 0.6,
         if ess <= threshold * n and temp != 1.0:
             eng.resample_tune(norm, float(rng.random()), copy=True)
             eng.refresh(full=True)
-            st = eng.rejuvenate(iterations=iterations, temperature=temp,
-                                seed=int(rng.integers(1 << 62)))
+            sweep = eng.mcmc_sweep if device_sweep else eng.rejuvenate
+            st = sweep(iterations=iterations, temperature=temp, seed=int(rng.integers(1 << 62)))
             moves["proposed"] += int(np.sum(st["proposed"]))
             moves["accepted"] += int(np.sum(st["accepted"]))
             if cat:

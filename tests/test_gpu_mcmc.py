@@ -393,11 +393,13 @@ def test_resample_tune_matches_oracle():
     eng.close()
 
 
-@pytest.mark.parametrize("reassign", ["gibbs", "learned"])
-def test_smc_driver_reaches_temperature_one(reassign):
+@pytest.mark.parametrize("reassign,device_sweep", [("gibbs", False), ("learned", False), ("learned", True)],
+                         ids=["gibbs-host", "learned-host", "learned-device"])
+def test_smc_driver_reaches_temperature_one(reassign, device_sweep):
     """The reference's SMC loop over the C-ABI (smccat.smc.run): temperatures
     rise monotonically to 1, resampling rounds happen, log Z is finite and the
-    particles keep exact likelihoods."""
+    particles keep exact likelihoods; rejuvenation host-driven or as the device
+    sweep."""
     from smccat import smc
     rng = np.random.default_rng(CFG.seed)
     codes, _ = workload.simulate_alignment(CFG, rng)
@@ -408,7 +410,7 @@ def test_smc_driver_reaches_temperature_one(reassign):
                       st["logits"], st["assign"], np.maximum(st["pinv"], 0.05), st["shape"])
     eng.refresh(full=True)
     res = smc.run(eng, cat=True, iterations=2, alg8_probability=0.5, reassign=reassign,
-                  learned_warmup=1, learned_updates=30, seed=4)
+                  learned_warmup=1, learned_updates=30, seed=4, device_sweep=device_sweep)
     temps = res["temperatures"]
     assert temps[-1] == 1.0 and all(b >= a for a, b in zip(temps, temps[1:]))
     assert res["resamples"] >= 1 and np.isfinite(res["log_z"])
