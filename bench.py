@@ -66,7 +66,7 @@ def parse():
                     help="also time the same particles with site-pattern compression")
     ap.add_argument("--mixed", type=int, default=1,
                     help="also time the FP32 (mixed-precision) path on the same particles")
-    ap.add_argument("--extra-configs", default="4",
+    ap.add_argument("--extra-configs", default="4,5",
                     help="comma-separated CAT configs (e.g. 3,4) to time in particle waves, at "
                          "their full particle counts ('' to skip)")
     ap.add_argument("--extra-particles", type=int, default=0,

@@ -310,6 +310,7 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
     }
 
     int nord = 0, nch = 0, local_k = -1;
+    unsigned long long rate_key = 0;
     double hastings = 0.0, dprior = 0.0;
     double new_pinv = a.hdr0[i].pinv;
     double new_rates[kMaxRates];
@@ -465,7 +466,9 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
                     double* ub = a.undo_base + (size_t)i * kBase;
                     for (int x = 0; x < kBase; ++x) ub[x] = bs[x];
                     if (kind == kRateFull) {
-                        for (int x = 0; x < kBase; ++x) zz[x] = curand_normal_double(&rs);
+                        // The 190 N(0, 1) draws come from a stream of their own,
+                        // keyed from this one, spread over the lanes below.
+                        rate_key = ((unsigned long long)curand(&rs) << 32) | curand(&rs);
                     } else {
                         const int x = min(kBase - 1, (int)(kBase * dm_unif(&rs)));
                         const double old = bs[x];
@@ -539,8 +542,14 @@ __global__ void __launch_bounds__(kDmWarps * 32) dm_propose_kernel(DmArgs a) {
     local_k = __shfl_sync(0xffffffffu, local_k, 0);
     __syncwarp();
     if (kind == kRateFull) {
-        // base += L z over the lanes (L lower triangular), and the N(0, 1)
-        // prior change of the exchangeabilities.
+        // z ~ N(0, I) (lane l draws z[l], z[l + 32], ... from subsequence l of
+        // the move's stream), then base += L z over the lanes (L lower
+        // triangular), and the N(0, 1) prior change of the exchangeabilities.
+        rate_key = __shfl_sync(0xffffffffu, rate_key, 0);
+        curandStatePhilox4_32_10_t zr;
+        curand_init(rate_key, (unsigned long long)lane, 0ull, &zr);
+        for (int x = lane; x < kBase; x += 32) zz[x] = curand_normal_double(&zr);
+        __syncwarp();
         double* bs = a.base + (size_t)i * kBase;
         double dp = 0.0;
         for (int x = lane; x < kBase; x += 32) {
@@ -1027,6 +1036,7 @@ using namespace smccat;
 extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, int32_t steps,
                                  double temperature, uint64_t seed, int32_t use_graph,
                                  int64_t* stats) {
+    NvtxRange range("smccat_tree_sweep");
     if (!c) return dm_fail(SMCCAT_EINVAL, "null context");
     unsigned long long ks[2 * kKinds];
     const int rc = device_sweep(c, first, count, steps, nullptr, temperature, seed, use_graph, ks);
@@ -1039,6 +1049,7 @@ extern "C" int smccat_tree_sweep(smccat_ctx* c, int32_t first, int32_t count, in
 extern "C" int smccat_mcmc_sweep(smccat_ctx* c, int32_t first, int32_t count, int32_t iterations,
                                  double temperature, uint64_t seed, int32_t use_graph,
                                  smccat_move_stats* stats) {
+    NvtxRange range("smccat_mcmc_sweep");
     if (!c) return dm_fail(SMCCAT_EINVAL, "null context");
     if (first < 0 || count < 1 || iterations < 0) return dm_fail(SMCCAT_EINVAL, "bad range");
     const Dims& d = dims_of(c);

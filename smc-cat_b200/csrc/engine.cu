@@ -592,6 +592,7 @@ int smccat_get_particles(smccat_ctx* c, int32_t first, int32_t count, int32_t* p
 }
 
 int smccat_refresh(smccat_ctx* c, int32_t first, int32_t count, int32_t mode) {
+    NvtxRange range("smccat_refresh");
     return refresh_internal(c, first, count, mode, nullptr);
 }
 
@@ -1153,6 +1154,7 @@ int smccat_accept(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* ma
 }
 
 int smccat_autotune(smccat_ctx* c, int32_t reps, int32_t* variant_out, double* ms_out) {
+    NvtxRange range("smccat_autotune");
     if (!c) return fail(SMCCAT_EINVAL, "null context");
     int n = 0;
     while (n < c->cfg.max_particles && c->slots[n].loaded) ++n;

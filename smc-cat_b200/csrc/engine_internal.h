@@ -10,11 +10,22 @@
 #include <vector>
 
 #include <omp.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "kernels.h"
 #include "smccat.h"
 
 namespace smccat {
+
+// A named NVTX range for the lifetime of the object: the entry points mark
+// their work for a profiler's timeline (no cost without one attached), where
+// the reference prints TIME_PROFILE timings (Particle.cpp:533-631).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Host loops over at least this many particles (state upload, plan packing,
 // proposals and MH tests) run on OpenMP threads; each iteration touches only

@@ -985,13 +985,10 @@ namespace {
 // Grid of the auxiliary-class kernel: kAuxCtasPerSm CTAs per SM, or fewer
 // when there are fewer tasks.
 int aux_grid(size_t tasks) {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
-            sms = 148;
-    }
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+        sms = 148;
     const size_t want = (tasks + kAuxWarps - 1) / kAuxWarps;
     const size_t cap = (size_t)sms * kAuxCtasPerSm;
     return (int)(want < cap ? (want > 0 ? want : 1) : cap);

@@ -335,6 +335,7 @@ int smccat_learned_gradients(smccat_ctx* c, int32_t n_sites, const int32_t* grou
 
 int smccat_learned_train(smccat_ctx* c, int32_t first, int32_t count, int32_t epochs,
                          int32_t batch_sites, double lr, uint64_t seed, double* loss_out) {
+    NvtxRange range("smccat_learned_train");
     if (!c || first < 0 || count < 1 || epochs < 0 || batch_sites < 1)
         return lfail(SMCCAT_EINVAL, "bad argument");
     if (!(model_flags_of(c) & SMCCAT_MODEL_CAT)) return lfail(SMCCAT_EINVAL, "the learned proposal needs SMCCAT_MODEL_CAT");

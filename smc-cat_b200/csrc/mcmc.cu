@@ -479,6 +479,7 @@ int smccat_set_split_posteriors(smccat_ctx* c, int32_t n, const uint64_t* bits, 
 
 int smccat_resample_tune(smccat_ctx* c, int32_t first, int32_t count, const double* w, double u,
                          int32_t copy, int32_t* anc_out) {
+    NvtxRange range("smccat_resample_tune");
     if (!c || !w || !anc_out) return mfail(SMCCAT_EINVAL, "null argument");
     if (first < 0 || count < 1) return mfail(SMCCAT_EINVAL, "bad range");
     if (!(u >= 0.0 && u < 1.0)) return mfail(SMCCAT_EINVAL, "u must be in [0, 1)");
@@ -670,6 +671,7 @@ int smccat_propose(smccat_ctx* c, int32_t p, int32_t family, uint64_t seed, int3
 
 int smccat_rejuvenate(smccat_ctx* c, int32_t first, int32_t count, int32_t iterations,
                       double temperature, uint64_t seed, smccat_move_stats* stats) {
+    NvtxRange range("smccat_rejuvenate");
     if (!c) return mfail(SMCCAT_EINVAL, "null context");
     if (iterations < 0 || count < 0 || first < 0) return mfail(SMCCAT_EINVAL, "bad range");
     const Dims& d = dims_of(c);
@@ -1118,10 +1120,21 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFreeAsync(dbuf, st);
     if (e != cudaSuccess) return mfail(SMCCAT_ECUDA, std::string("gibbs: ") + cudaGetErrorString(e));
+    // The table's pruning launches report through the engine's status word:
+    // read and clear it here, so that it neither leaks into the next refresh
+    // nor goes unreported.
+    if (use_table) {
+        int es = 0;
+        e = cudaMemcpy(&es, view.status, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && es) e = cudaMemset(view.status, 0, sizeof(int));
+        if (e != cudaSuccess) return mfail(SMCCAT_ECUDA, std::string("gibbs: ") + cudaGetErrorString(e));
+        if (es & 2) status |= 8;
+    }
     if (lstats) {
         *lstats = smccat_learned_stats{};
         for (int j = 0; j < n; ++j) { lstats->proposed += nprop[j]; lstats->accepted += nacc[j]; }
     }
+    if (status & 8) return mfail(SMCCAT_ETIMEOUT, "a bounded device wait gave up during the reassignment");
     if (site >= 0) {
         const int K = slot_of(c, list[0]).cur.K;
         for (int k = 0; k < K; ++k) weights_out[k] = wout[k];
@@ -1129,7 +1142,6 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
             for (int j = 0; j < naux; ++j) weights_out[K + j] = wout[K + j];
         return SMCCAT_OK;
     }
-    if (status & 8) return mfail(SMCCAT_ETIMEOUT, "a bounded wait in the learned move gave up");
     if (status & 4) return mfail(SMCCAT_ENOMEM, "Gibbs reassignment ran out of class slots");
     // Compact the surviving classes and install the new assignments
     // (the reference erases empty classes as it goes, Particle.cpp:817-821).
@@ -1177,6 +1189,7 @@ extern "C" {
 
 int smccat_gibbs(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* mask, double temperature,
                  uint64_t seed, smccat_gibbs_stats* stats) {
+    NvtxRange range("smccat_gibbs");
     if (!c || first < 0 || count < 0) return mfail(SMCCAT_EINVAL, "bad argument");
     if (!(model_flags_of(c) & SMCCAT_MODEL_CAT)) return mfail(SMCCAT_EINVAL, "Gibbs reassignment needs SMCCAT_MODEL_CAT");
     std::vector<int> list;
@@ -1193,6 +1206,7 @@ int smccat_gibbs(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* mas
 int smccat_learned_move(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* mask,
                         int32_t updates, double temperature, uint64_t seed,
                         smccat_learned_stats* stats) {
+    NvtxRange range("smccat_learned_move");
     if (!c || first < 0 || count < 0 || updates < 1) return mfail(SMCCAT_EINVAL, "bad argument");
     if (!(model_flags_of(c) & SMCCAT_MODEL_CAT)) return mfail(SMCCAT_EINVAL, "the learned move needs SMCCAT_MODEL_CAT");
     if (dims_of(c).R > 2 * 4) return mfail(SMCCAT_EINVAL, "the learned move supports at most 8 rates");
@@ -1229,6 +1243,7 @@ int smccat_gibbs_weights(smccat_ctx* c, int32_t p, int32_t site, const double* a
 int smccat_smc_step(smccat_ctx* c, int32_t first, int32_t count, double* raw_weights,
                     double target_ess, double last_temp, double* cur_temp, double* ess,
                     double* norm_weights) {
+    NvtxRange range("smccat_smc_step");
     if (!c || !raw_weights || !cur_temp || !ess || !norm_weights || count < 1 || first < 0)
         return mfail(SMCCAT_EINVAL, "bad argument");
     void* stv = nullptr;

@@ -6,7 +6,8 @@
   SMCCAT_ETIMEOUT -- the kernels drain the copies they still have in flight
   and return -- and, with the default limit restored, the next refresh must
   match the oracle again. Nothing waits on a flag that is never set: the
-  copies really complete; only the poll budget is zero.
+  copies really complete; only the poll budget is zero. The learned move's
+  tensor-core product waits go through the same knob.
 * Non-finite state: a NaN in one particle's exchangeabilities, made on the
   host before upload, must surface as SMCCAT_ENUMERIC (the reference aborts on
   a NaN ESS instead, main.cpp:158-174), with that particle's log-likelihood NaN
@@ -89,4 +90,32 @@ def test_nan_state_reports_enumeric():
     _load(eng, st)
     eng.refresh(full=True)
     np.testing.assert_allclose(eng.lnl(), _oracle(codes, st), rtol=1e-9, atol=0)
+    eng.close()
+
+
+def test_learned_move_wait_timeout_reports_and_recovers():
+    """The learned move's tcgen05 products are waited on with the same bounded
+    polls: with a zero budget the move stops at its first product, drains it,
+    releases its tensor memory and reports SMCCAT_ETIMEOUT with the particles'
+    assignments untouched; with the default budget the next move runs and the
+    likelihoods stay exact."""
+    eng, codes, st = _setup()
+    _load(eng, st)
+    eng.refresh(full=True)
+    eng.learned_params(set_to=(np.random.default_rng(2).normal(size=smccat.MLP_PARAMS) * 0.1)
+                       .astype(np.float32))
+    before = eng.get_particles()["assign"].copy()
+    eng.set_wait_limit(0)
+    with pytest.raises(smccat.SmccatError) as err:
+        eng.learned_move(updates=20, temperature=1.0, seed=3)
+    assert err.value.code == smccat.ETIMEOUT
+    np.testing.assert_array_equal(eng.get_particles()["assign"], before)
+    eng.set_wait_limit(-1)
+    eng.refresh(full=True)
+    eng.learned_move(updates=50, temperature=1.0, seed=4)
+    fin = eng.get_particles()
+    rates = np.stack([oracle.discretize_gamma(s, CFG.R) for s in fin["shape"]])
+    ref = oracle.lnl_batch(codes, fin["parent"], fin["branch"], fin["base"], fin["num_classes"],
+                           fin["logits"], fin["assign"], fin["pinv"], rates)
+    np.testing.assert_allclose(eng.lnl(), ref, rtol=1e-9, atol=0)
     eng.close()
