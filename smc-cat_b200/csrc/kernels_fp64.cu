@@ -280,7 +280,11 @@ __global__ void __launch_bounds__(kPmThreads) pmat_kernel(const PmJob* __restric
 // still in flight (waiting on its un-toggled parity, with the full limit)
 // before the buffers are reused. Returns false, uniformly across the CTA,
 // when any warp gave up.
-template <class T, int R, int MINB, int W, int RB>
+// EV: the instance for evaluation mode (PruneArgs::eval_k / eval_kp and the
+// site lists). The refresh instance keeps only the eval_k test: without the
+// site-list and per-particle code its register allocation spills less
+// (20 / 12 bytes instead of 44 / 56 at <double, 4, 3, 1, 4>).
+template <class T, int R, int MINB, int W, int RB, bool EV>
 __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id, uint32_t& phase, bool init) {
     const Dims d = a.d;
     const Tile tl = a.tiles[tile_id];
@@ -293,14 +297,17 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     __shared__ int bad;
 
     const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
-    // The class whose matrices and frequencies the tile runs: its own, or the
-    // class under evaluation.
-    const int ek = a.eval_kp ? a.eval_kp[p - a.first] : a.eval_k;
-    const int kc = ek >= 0 ? ek : tl.k;
-    // Evaluation over a site list: the tile's slots stand for listed sites.
-    const bool listed = ek >= 0 && a.eval_perm != nullptr;
-    const int nsl = listed ? min(tl.nslots, a.eval_nv[p - a.first] - tl.slot0) : tl.nslots;
-    const int32_t* sperm = listed ? a.eval_perm + (size_t)(p - a.first) * d.S : a.perm + (size_t)p * d.S;
+    // Evaluation mode: the class under evaluation and, over a site list, the
+    // sites the tile's slots stand for.
+    int nsl = tl.nslots;
+    const int32_t* sperm = a.perm + (size_t)p * d.S;
+    if constexpr (EV) {
+        const int ek0 = a.eval_kp ? a.eval_kp[p - a.first] : a.eval_k;
+        if (ek0 >= 0 && a.eval_perm != nullptr) {
+            nsl = min(tl.nslots, a.eval_nv[p - a.first] - tl.slot0);
+            sperm = a.eval_perm + (size_t)(p - a.first) * d.S;
+        }
+    }
     const bool valid = lane < nsl;  // the lane owns at least one slot
     // A lane's unused slots alias its first slot (or the tile's first): they
     // are computed like the others and never stored.
@@ -328,6 +335,10 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     const size_t lws_stride = j_stride;
     T* CLp = static_cast<T*>(a.CL) + (size_t)p * d.NI * node_stride;
     double* LSCp = a.LSC + (size_t)p * d.NI * 2 * lws_stride;
+    // The class whose matrices and frequencies the tile runs: its own, or the
+    // class under evaluation.
+    const int ek = EV ? (a.eval_kp ? a.eval_kp[p - a.first] : a.eval_k) : a.eval_k;
+    const int kc = ek >= 0 ? ek : tl.k;
     const T* Pcls = static_cast<const T*>(a.Pm) +
                     ((size_t)p * d.Kmax + kc) * d.N * 2 * (size_t)R * kPBlock + (size_t)r * kPBlock;
     auto pblock = [&](int child, int pws) {
@@ -343,9 +354,10 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     __syncthreads();
     if (!h->active) return true;  // uniform across the CTA (after the barriers exist)
     const int ej = ek >= 0 ? a.eval_map[p - a.first] : 0;
-    if (a.eval_kp ? (ek < 0 || ej < 0) : (ek >= 0 && (ej < 0 || ek >= h->num_classes)))
+    if (EV ? (a.eval_kp ? (ek < 0 || ej < 0) : (ek < 0 || ej < 0 || ek >= h->num_classes))
+           : (ek >= 0 && (ej < 0 || ek >= h->num_classes)))
         return true;  // uniform as well
-    if (ek >= 0 && nsl <= 0) return true;  // past the end of the site list
+    if (EV && nsl <= 0) return true;  // past the end of the site list
 
     // A class-local refresh of another class leaves this tile's partials as
     // they are: only its root reduction reruns. In evaluation mode the plan
@@ -584,22 +596,22 @@ __device__ __forceinline__ bool prune_tile(const PruneArgs& a, const int tile_id
     return tile_ok;
 }
 
-template <class T, int R, int MINB, int W, int RB>
+template <class T, int R, int MINB, int W, int RB, bool EV>
 __global__ void __launch_bounds__(32 * R, MINB) prune_kernel(const PruneArgs a) {
     uint32_t phase = 0;
-    prune_tile<T, R, MINB, W, RB>(a, a.tile_begin + blockIdx.x, phase, true);
+    prune_tile<T, R, MINB, W, RB, EV>(a, a.tile_begin + blockIdx.x, phase, true);
 }
 
 // Persistent form: one wave of CTAs (the SMs times the CTAs each holds) walks
 // the tiles in a grid-stride loop. The copy barriers are initialised once and
 // their phases carried from tile to tile; every copy a tile issues is waited
 // on inside that tile.
-template <class T, int R, int MINB, int W, int RB>
+template <class T, int R, int MINB, int W, int RB, bool EV>
 __global__ void __launch_bounds__(32 * R, MINB) prune_kernel_persistent(const PruneArgs a, int ntiles) {
     uint32_t phase = 0;
     bool init = true;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const bool ok = prune_tile<T, R, MINB, W, RB>(a, a.tile_begin + t, phase, init);
+        const bool ok = prune_tile<T, R, MINB, W, RB, EV>(a, a.tile_begin + t, phase, init);
         init = false;
         __syncthreads();
         if (!ok) break;  // a wait gave up: the CTA's remaining tiles stay unevaluated (status bit 2)
@@ -652,7 +664,8 @@ namespace {
 template <class T, int R, int MINB, int W, int RB>
 cudaError_t launch_prune_persistent_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
     const size_t smem = sizeof(T) * 4 * (size_t)kPBlock * R;
-    auto k = prune_kernel_persistent<T, R, MINB, W, RB>;
+    const bool ev = a.eval_k >= 0 || a.eval_kp != nullptr;
+    auto k = ev ? prune_kernel_persistent<T, R, MINB, W, RB, true> : prune_kernel_persistent<T, R, MINB, W, RB, false>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
@@ -667,13 +680,14 @@ cudaError_t launch_prune_persistent_t(const PruneArgs& a, int ntiles, cudaStream
 template <class T, int R, int MINB, int W, int RB>
 cudaError_t launch_prune_t(const PruneArgs& a, int ntiles, cudaStream_t st) {
     const size_t smem = sizeof(T) * 4 * (size_t)kPBlock * R;
-    cudaError_t e = cudaFuncSetAttribute(prune_kernel<T, R, MINB, W, RB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const bool ev = a.eval_k >= 0 || a.eval_kp != nullptr;
+    auto k = ev ? prune_kernel<T, R, MINB, W, RB, true> : prune_kernel<T, R, MINB, W, RB, false>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     // The shared-memory carveout stays at the driver's choice: forcing the
     // maximum (room for a fourth CTA's P buffers) measured slower, since the
     // register-capped variants' spills then miss the smaller L1.
-    prune_kernel<T, R, MINB, W, RB><<<ntiles, 32 * R, smem, st>>>(a);
+    k<<<ntiles, 32 * R, smem, st>>>(a);
     return cudaGetLastError();
 }
 
