@@ -383,10 +383,14 @@ typedef struct smccat_gibbs_stats {
  * (Particle.cpp:785-995, main.cpp:303-306) for the particles of
  * [first, first+count) whose mask byte is non-zero (mask may be NULL = all):
  * Neal's Algorithm 8 with m = 5 auxiliary classes, floor(S/2) random-site
- * iterations per particle, run on the device, one thread block per particle.
- * Emptied classes are removed and the survivors renumbered in order; new
- * classes are appended. Needs SMCCAT_MODEL_CAT and no pending edits; fails
- * with SMCCAT_ENOMEM if a particle would exceed max_classes. */
+ * iterations per particle, run on the device: every iteration's auxiliary
+ * classes evaluated at once, then each particle's iterations in order with the
+ * classes' site log-likelihoods from a table the pruning kernels fill. The
+ * particles run in groups sized to half the free device memory (the result
+ * does not depend on the grouping). Emptied classes are removed and the
+ * survivors renumbered in order; new classes are appended. Needs
+ * SMCCAT_MODEL_CAT and no pending edits; fails with SMCCAT_ENOMEM if a
+ * particle would exceed max_classes. */
 int smccat_gibbs(smccat_ctx* ctx, int32_t first, int32_t count, const uint8_t* mask,
                  double temperature, uint64_t seed, smccat_gibbs_stats* stats);
 
@@ -502,6 +506,12 @@ int smccat_set_kernel_variant(smccat_ctx* ctx, int32_t variant);
  * without stalling or faulting the device. No counterpart in the reference
  * (it has no device code). */
 int smccat_set_wait_limit(smccat_ctx* ctx, int32_t polls);
+
+/* Particles per device pass of smccat_gibbs / smccat_learned_move: n > 0 fixes
+ * the group size, n <= 0 restores the default (groups sized to half the free
+ * device memory). The results do not depend on it. No counterpart in the
+ * reference. */
+int smccat_set_reassign_group(smccat_ctx* ctx, int32_t n);
 
 /* Enable (1) or disable (0) per-launch CUDA-event timing; resets counters. */
 int smccat_set_profiling(smccat_ctx* ctx, int32_t enable);

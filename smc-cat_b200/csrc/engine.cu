@@ -85,6 +85,7 @@ struct smccat_ctx {
     int tile_cap = 0;
     int prune_variant = 0;      // chosen by smccat_autotune
     uint32_t wait_limit = kDrainPolls;  // polls per bounded device wait (smccat_set_wait_limit)
+    int reassign_group = 0;             // particles per reassignment pass (0: from free memory)
     int tile_sites = kTileSites;  // slots per pruning tile, as the variant expects
 
     std::vector<uint8_t> codes;
@@ -950,6 +951,8 @@ int smccat::device_view(smccat_ctx* c, int first, int count, DeviceView* v) {
 const Dims& smccat::dims_of(const smccat_ctx* c) { return c->d; }
 int smccat::model_flags_of(const smccat_ctx* c) { return c->cfg.model_flags; }
 uint32_t smccat::wait_limit_of(const smccat_ctx* c) { return c->wait_limit; }
+int smccat::device_of(const smccat_ctx* c) { return c->cfg.device; }
+int smccat::reassign_group_of(const smccat_ctx* c) { return c->reassign_group; }
 const double* smccat::lnl_device(const smccat_ctx* c) { return c->d_lnl; }
 const uint8_t* smccat::codes_device(const smccat_ctx* c) { return c->d_codes; }
 const uint8_t* smccat::codes_host(const smccat_ctx* c) { return c->codes.data(); }
@@ -1213,6 +1216,12 @@ int smccat_set_kernel_variant(smccat_ctx* c, int32_t variant) {
 int smccat_set_wait_limit(smccat_ctx* c, int32_t polls) {
     if (!c) return fail(SMCCAT_EINVAL, "null context");
     c->wait_limit = polls < 0 ? kDrainPolls : static_cast<uint32_t>(polls);
+    return SMCCAT_OK;
+}
+
+int smccat_set_reassign_group(smccat_ctx* c, int32_t n) {
+    if (!c) return fail(SMCCAT_EINVAL, "null context");
+    c->reassign_group = n > 0 ? n : 0;
     return SMCCAT_OK;
 }
 

@@ -82,6 +82,8 @@ int particles_of(const smccat_ctx* c);  // particle slots of the context
 const Dims& dims_of(const smccat_ctx* c);
 int model_flags_of(const smccat_ctx* c);
 uint32_t wait_limit_of(const smccat_ctx* c);  // polls per bounded device wait
+int device_of(const smccat_ctx* c);            // the context's CUDA device
+int reassign_group_of(const smccat_ctx* c);    // smccat_set_reassign_group (0: default)
 const double* lnl_device(const smccat_ctx* c);  // [max_particles] current log-likelihoods
 const uint8_t* codes_device(const smccat_ctx* c);   // [T][S]
 const double* isinv_device(const smccat_ctx* c);    // [S]

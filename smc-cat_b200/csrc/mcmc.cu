@@ -1187,6 +1187,30 @@ int run_gibbs(smccat_ctx* c, const std::vector<int>& list, double temperature, u
 
 extern "C" {
 
+}  // extern "C"
+
+namespace {
+
+// Particles per reassignment call: the call's device buffers, dominated by the
+// class table (Kmax x S doubles per particle), take at most half of the free
+// device memory. A pass's random streams are keyed by particle, so splitting
+// the particles into calls changes nothing in the result.
+size_t reassign_chunk(const smccat_ctx* c) {
+    if (reassign_group_of(c) > 0) return (size_t)reassign_group_of(c);
+    const Dims& d = dims_of(c);
+    size_t freeb = 0, total = 0;
+    if (cudaSetDevice(device_of(c)) != cudaSuccess || cudaMemGetInfo(&freeb, &total) != cudaSuccess ||
+        freeb == 0)
+        return 1;
+    const size_t per = (size_t)d.Kmax * d.S * 8 + (size_t)d.S * 64 +
+                       (size_t)(d.Kmax + 64 + gibbs_aux()) * (kSpecStride + 2 * kStates) * 8 + (size_t)1 << 20;
+    return std::max<size_t>(1, freeb / 2 / per);
+}
+
+}  // namespace
+
+extern "C" {
+
 int smccat_gibbs(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* mask, double temperature,
                  uint64_t seed, smccat_gibbs_stats* stats) {
     NvtxRange range("smccat_gibbs");
@@ -1200,7 +1224,21 @@ int smccat_gibbs(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* mas
         if (s.pending) return mfail(SMCCAT_ESTATE, "particle has uncommitted edits");
         list.push_back(first + i);
     }
-    return run_gibbs(c, list, temperature, seed, -1, nullptr, nullptr, stats);
+    const size_t chunk = reassign_chunk(c);
+    smccat_gibbs_stats total{};
+    for (size_t b = 0; b < list.size() || b == 0; b += chunk) {
+        const std::vector<int> part(list.begin() + b, list.begin() + std::min(list.size(), b + chunk));
+        smccat_gibbs_stats gs{};
+        const int rc = run_gibbs(c, part, temperature, seed, -1, nullptr, nullptr, &gs);
+        if (rc) return rc;
+        total.particles += gs.particles;
+        total.classes_before += gs.classes_before;
+        total.classes_after += gs.classes_after;
+        total.created += gs.created;
+        if (list.empty()) break;
+    }
+    if (stats) *stats = total;
+    return SMCCAT_OK;
 }
 
 int smccat_learned_move(smccat_ctx* c, int32_t first, int32_t count, const uint8_t* mask,
@@ -1218,7 +1256,19 @@ int smccat_learned_move(smccat_ctx* c, int32_t first, int32_t count, const uint8
         if (s.pending) return mfail(SMCCAT_ESTATE, "particle has uncommitted edits");
         list.push_back(first + i);
     }
-    return run_gibbs(c, list, temperature, seed, -1, nullptr, nullptr, nullptr, updates, stats);
+    const size_t chunk = reassign_chunk(c);
+    smccat_learned_stats total{};
+    for (size_t b = 0; b < list.size() || b == 0; b += chunk) {
+        const std::vector<int> part(list.begin() + b, list.begin() + std::min(list.size(), b + chunk));
+        smccat_learned_stats ls{};
+        const int rc = run_gibbs(c, part, temperature, seed, -1, nullptr, nullptr, nullptr, updates, &ls);
+        if (rc) return rc;
+        total.proposed += ls.proposed;
+        total.accepted += ls.accepted;
+        if (list.empty()) break;
+    }
+    if (stats) *stats = total;
+    return SMCCAT_OK;
 }
 
 int smccat_learned_scores(smccat_ctx* c, int32_t p, int32_t site, double* out) {

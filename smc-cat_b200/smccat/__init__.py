@@ -126,6 +126,7 @@ def lib():
         "smccat_kernel_variants": ([vp, _ip, _ip], ctypes.c_int),
         "smccat_set_kernel_variant": ([vp, _i32], ctypes.c_int),
         "smccat_set_wait_limit": ([vp, _i32], ctypes.c_int),
+        "smccat_set_reassign_group": ([vp, _i32], ctypes.c_int),
         "smccat_set_tuning": ([vp, ctypes.POINTER(Tuning)], ctypes.c_int),
         "smccat_get_tuning": ([vp, ctypes.POINTER(Tuning)], ctypes.c_int),
         "smccat_set_rate_cholesky": ([vp, _dp], ctypes.c_int),
@@ -532,6 +533,10 @@ class Engine:
     def set_wait_limit(self, polls: int):
         """Polls per bounded device wait; a negative value restores the default."""
         _check(lib().smccat_set_wait_limit(self._h, int(polls)))
+
+    def set_reassign_group(self, n: int):
+        """Particles per device pass of Gibbs / the learned move (0: from free memory)."""
+        _check(lib().smccat_set_reassign_group(self._h, int(n)))
 
     def set_profiling(self, enable: bool):
         _check(lib().smccat_set_profiling(self._h, 1 if enable else 0))

@@ -448,3 +448,33 @@ def test_gibbs_class_table_matches_per_site_evaluation():
     np.testing.assert_array_equal(a["num_classes"], b["num_classes"])
     np.testing.assert_array_equal(a["assign"], b["assign"])
     np.testing.assert_allclose(la, lb, rtol=1e-12)
+
+
+def test_reassignment_groups_do_not_change_results():
+    """Gibbs and the learned move run their particles in device passes sized
+    to the free memory; the random streams are keyed by particle, so passes
+    of two particles give the same assignments and likelihoods as one pass of
+    all of them."""
+    cfg = workload.WorkloadConfig("groups", T=10, S=300, R=4, particles=6, iterations=1,
+                                  lg=False, invar=True, cat=True, pinv=0.1, k_range=(2, 7), seed=72)
+    rng = np.random.default_rng(cfg.seed)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    st = workload.make_particles(cfg, cfg.particles, rng, kmax=24)
+    params = (np.random.default_rng(8).normal(size=smccat.MLP_PARAMS) * 0.1).astype(np.float32)
+    out = []
+    for group in (0, 2):
+        eng = smccat.Engine(codes, cfg.R, cfg.particles, max_classes=24, invar=True, cat=True)
+        eng.set_reassign_group(group)
+        eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                          st["logits"], st["assign"], st["pinv"], st["shape"])
+        eng.refresh(full=True)
+        g = eng.gibbs(temperature=0.8, seed=21)
+        eng.learned_params(set_to=params)
+        lm = eng.learned_move(updates=100, temperature=0.8, seed=22)
+        out.append((eng.get_particles(), eng.lnl(), g, lm))
+        eng.close()
+    (a, la, ga, ma), (b, lb, gb, mb) = out
+    assert ga == gb and ma == mb
+    np.testing.assert_array_equal(a["num_classes"], b["num_classes"])
+    np.testing.assert_array_equal(a["assign"], b["assign"])
+    np.testing.assert_allclose(la, lb, rtol=1e-12)
