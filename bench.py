@@ -84,6 +84,10 @@ def parse():
                          "CAT workload: plain FP64 + Gibbs against FP32 + learned proposal, "
                          "this many replicate seeds each")
     ap.add_argument("--smc-particles", type=int, default=64)
+    ap.add_argument("--smc-iterations", type=int, default=5,
+                    help="rejuvenation iterations per resampling round of the --smc analyses")
+    ap.add_argument("--smc-alg8", type=float, default=0.1,
+                    help="fraction of particles given a class reassignment per round (alg8Probability)")
     ap.add_argument("--gibbs-particles", type=int, default=0,
                     help="particles of a CAT --extra-configs run timed through one Gibbs pass "
                          "and one learned-proposal pass (0 to skip)")
@@ -459,7 +463,7 @@ def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=10, chosen_sweeps=
     return res
 
 
-def measure_smc(reps, n, local, torch):
+def measure_smc(reps, n, local, torch, iterations=5, alg8=0.1):
     """Whole SMC analyses (main.cpp:147-336 through smccat.smc.run) from the
     same initial population, per arm and replicate seed (plain: FP64, host
     lockstep rejuvenation, Gibbs; chosen: FP32, the device sweep, the learned
@@ -470,7 +474,7 @@ def measure_smc(reps, n, local, torch):
     import smccat
     from smccat import smc, workload
     cfg = workload.WorkloadConfig("cat_gtr_g4_16x500", T=16, S=500, R=4, particles=n,
-                                  iterations=5, lg=False, invar=False, cat=True, alpha=0.8,
+                                  iterations=iterations, lg=False, invar=False, cat=True, alpha=0.8,
                                   dp_concentration=3.0, k_range=(1, 6), seed=9)
     codes, _ = workload.simulate_alignment(cfg, np.random.default_rng(cfg.seed))
     st = workload.make_particles(cfg, n, np.random.default_rng(99))
@@ -478,7 +482,7 @@ def measure_smc(reps, n, local, torch):
     logits = np.zeros((n, kmax, 20))
     logits[:, :st["logits"].shape[1]] = st["logits"]
     out = {"workload": cfg.name, "particles": n, "rejuvenation_iterations": cfg.iterations,
-           "threshold": 0.6, "alg8_probability": 0.1}
+           "threshold": 0.6, "alg8_probability": alg8}
     for arm, prec, move, dev in (("plain_fp64_gibbs", smccat.PREC_FP64, "gibbs", False),
                                  ("fp32_learned", smccat.PREC_FP32, "learned", True)):
         runs = []
@@ -489,7 +493,7 @@ def measure_smc(reps, n, local, torch):
                               logits, st["assign"], st["pinv"], st["shape"])
             eng.refresh(full=True)
             res = smc.run(eng, cat=True, iterations=cfg.iterations, reassign=move, seed=1000 + r,
-                          sync=torch.cuda.synchronize, device_sweep=dev)
+                          alg8_probability=alg8, sync=torch.cuda.synchronize, device_sweep=dev)
             res.pop("temperatures")
             runs.append(res)
             eng.close()
@@ -963,7 +967,8 @@ def main():
                                      gibbs_particles=args.gibbs_particles)
                 for c in args.extra_configs.split(",") if c.strip()]
         if args.smc:
-            line["smc"] = measure_smc(args.smc, args.smc_particles, local, torch)
+            line["smc"] = measure_smc(args.smc, args.smc_particles, local, torch,
+                                      iterations=args.smc_iterations, alg8=args.smc_alg8)
         if args.sampler_config:
             line["sampler"] = measure_sampler(args.sampler_config, args.sampler_particles,
                                               args.sampler_sweeps, local, torch,
