@@ -332,7 +332,8 @@ def multichain_ess(x):
 
 
 def measure_sampler(cid, n, sweeps, local, torch, gibbs_every=10, chosen_sweeps=10):
-    """The north-star sampler comparison on a CAT configuration.
+    """The sampler comparison (plain FP64 path against the mixed-precision,
+    graph-captured, learned-proposal sampler) on a CAT configuration.
 
     One sweep = Mcmc::operator() with the configuration's iterations on every
     particle + one CAT reassignment pass of floor(S/2) site updates per
