@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(32 * kGibbsWarps) gibbs_kernel(GibbsArgs a) {
     const bool tabmode = a.table != nullptr;
     const int it0 = tabmode ? a.resume_it[i] : 0;
     const int kstart = tabmode ? a.resume_kcur[i] : gp.K;
-    if (it0 >= gp.n_iter) return;  // finished in an earlier round (uniform)
+    if (it0 > 0 && it0 >= gp.n_iter) return;  // finished in an earlier round (uniform)
     if (threadIdx.x == 0) s_kcur = kstart;
     for (int k = threadIdx.x; k < Kcap + kAux; k += blockDim.x) counts[k] = 0;
     __syncthreads();

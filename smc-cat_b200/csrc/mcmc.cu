@@ -1203,7 +1203,8 @@ size_t reassign_chunk(const smccat_ctx* c) {
         freeb == 0)
         return 1;
     const size_t per = (size_t)d.Kmax * d.S * 8 + (size_t)d.S * 64 +
-                       (size_t)(d.Kmax + 64 + gibbs_aux()) * (kSpecStride + 2 * kStates) * 8 + (size_t)1 << 20;
+                       (size_t)(d.Kmax + 64 + gibbs_aux()) * (kSpecStride + 2 * kStates) * 8 +
+                       ((size_t)1 << 20);
     return std::max<size_t>(1, freeb / 2 / per);
 }
 

@@ -478,3 +478,25 @@ def test_reassignment_groups_do_not_change_results():
     np.testing.assert_array_equal(a["num_classes"], b["num_classes"])
     np.testing.assert_array_equal(a["assign"], b["assign"])
     np.testing.assert_allclose(la, lb, rtol=1e-12)
+
+
+def test_gibbs_with_no_site_iterations():
+    """floor(S/2) = 0 iterations (a one-site alignment): the pass leaves every
+    particle as it was, with its likelihood exact."""
+    cfg = workload.WorkloadConfig("one_site", T=6, S=1, R=4, particles=3, iterations=1,
+                                  lg=True, invar=False, cat=True, k_range=(1, 1), seed=5)
+    rng = np.random.default_rng(cfg.seed)
+    codes, _ = workload.simulate_alignment(cfg, rng)
+    st = workload.make_particles(cfg, cfg.particles, rng, kmax=4)
+    eng = smccat.Engine(codes, cfg.R, cfg.particles, max_classes=4, lg=True, cat=True)
+    eng.set_particles(0, st["parent"], st["branch"], st["base"], st["num_classes"],
+                      st["logits"], st["assign"], st["pinv"], st["shape"])
+    eng.refresh(full=True)
+    before = eng.lnl().copy()
+    res = eng.gibbs(temperature=1.0, seed=3)
+    assert res["particles"] == cfg.particles and res["created"] == 0
+    fin = eng.get_particles()
+    np.testing.assert_array_equal(fin["num_classes"], st["num_classes"])
+    np.testing.assert_array_equal(fin["assign"], st["assign"])
+    np.testing.assert_allclose(eng.lnl(), before, rtol=1e-12)
+    eng.close()
